@@ -1,0 +1,380 @@
+"""Benchmark: phase-space DOF-updates/s of the SSP-RK3 step (FP64 plain and FP32 mixed).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the medium benchmark configuration): Nx = 32, Nu = Nv = 50 elements, LGL order 8
+(256 x 400 x 400 = 40.96M DOF), loss cone j = 6, perturbation 1e-3 cos kx plus seeded 1e-6
+noise per x node, reference normalisation (omega_p / omega_c = 10, k = 0.886 gyroradius
+units).  One step = one nonlinear SSP-RK3 step: 3 fused stage kernels + 3 field kernels.
+Each state buffer (377 MB FP64 / 189 MB FP32) is larger than the 126 MB L2, so no flush is
+needed between steps.  With N > 1 ranks (torchrun) every GPU advances its own replica (the
+solver is single-GPU; replicas only): ``value`` is the sum over ranks, times are the max.
+
+Prints ONE JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "phase-space DOF-updates/s per RK3 step, FP64 plain vs FP32 mixed; HBM roofline %"
+RES = (32, 50, 50)
+ORDER = 8
+SAMPLE_RES = (4, 50, 50)  # CPU sample: the same velocity grid, 4 of the 32 x elements
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-reps", type=int, default=10)
+    return ap.parse_args()
+
+
+def dof(res, n):
+    return res[0] * res[1] * res[2] * n ** 3
+
+
+# ----------------------------------------------------------------------------------------------
+# CPU (oracle port) timing: the reference arm and the cpu_baseline object
+# ----------------------------------------------------------------------------------------------
+def cpu_port_rate(steps, warmup):
+    import numpy as np
+
+    from oracle import vlasov_oracle as vo
+
+    c = vo.make_case(*SAMPLE_RES, ORDER)
+    f = vo.cos_perturbed(c, c.extra["norm"].vt_e, 6, 1.0e-3, noise=1.0e-6, seed=0)
+    rho = vo.moment_zero(f, c)
+    E0, _ = vo.poisson2(rho - np.mean(rho), c)
+    dt = vo.adapt_dt(E0, c)
+    for _ in range(warmup):
+        _, dt = vo.ssp_rk3_step(f, dt, c)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _, dt = vo.ssp_rk3_step(f, dt, c)
+    t = (time.perf_counter() - t0) / max(steps, 1)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return dof(SAMPLE_RES, ORDER) / t, t, cores
+
+
+def cpu_baseline_obj(steps=3, warmup=1):
+    rate, t, cores = cpu_port_rate(steps, warmup)
+    return {"value": rate, "unit": "DOF-updates/s", "cores": cores, "kind": "port",
+            "sample": f"oracle (NumPy FP64 restatement of the reference step) on Nx={SAMPLE_RES[0]}, "
+                      f"Nu=Nv={SAMPLE_RES[1]}, n={ORDER} ({dof(SAMPLE_RES, ORDER)/1e6:.2f}M DOF), "
+                      f"{steps} steps after {warmup} warm-up, {t:.2f} s/step; BLAS threads = cores, "
+                      "elementwise NumPy single-threaded"}
+
+
+# ----------------------------------------------------------------------------------------------
+# clocks sampling (nvidia-smi during the timed region)
+# ----------------------------------------------------------------------------------------------
+class Clocks:
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"vl_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ----------------------------------------------------------------------------------------------
+# GPU measurement
+# ----------------------------------------------------------------------------------------------
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except Exception:
+        return 6650.0, "fallback 6.65 TB/s (of fallback)"
+
+
+def measure_precision(precision, steps, warmup, reps, dist):
+    import torch
+
+    from vlasov1d2v_b200 import problem
+    from vlasov1d2v_b200.timestep import _BIG_STEPS, get_max_speeds
+
+    p = problem.build(RES, ORDER, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=0,
+                      precision=precision, batch_steps=max(steps, warmup, 1))
+    st = p.stepper
+    st.adapt_time_step(max_speeds=get_max_speeds(p.grids, p.elliptic, p.refs),
+                       dx=p.grids.x.dx, du=p.grids.u.dx, dv=p.grids.v.dx)
+    run = st._run(p.f, p.elliptic, p.grids, p.refs)
+    run.upload_state(st._host_state(run, float("inf"), _BIG_STEPS))
+    n_dof = dof(RES, ORDER)
+    es = 8 if precision == "fp64" else 4
+
+    # warm-up (eager), then capture the K-step graph
+    if warmup:
+        run.launch(warmup, use_graph=False)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            run.ctx.ssp_rk3_steps(run.f, run.sa, run.sb, run.E, run.phi, run.state, steps)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record()
+    g.replay()
+    ev1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    stt = run.read_state()
+    if stt.status != 0:
+        raise RuntimeError("non-finite state during the benchmark")
+
+    # per-kernel timing of the three stage kinds (the dominant kernel) with CUDA events
+    ctx = run.ctx
+    dt_t = torch.tensor([float(stt.dt)], dtype=torch.float64, device=run.f.device)
+    stage_ms = []
+    for stage, inp, fn, out in ((0, run.f, None, run.sa), (1, run.sa, run.f, run.sb),
+                                (2, run.sb, run.f, run.sa)):
+        for _ in range(2):
+            ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
+        b.record()
+        torch.cuda.synchronize()
+        stage_ms.append(a.elapsed_time(b) / reps)
+    # field kernel (single CTA Poisson solve from a density)
+    rho = torch.zeros((RES[0], ORDER), dtype=torch.float64, device=run.f.device)
+    ctx.moment(run.f, rho)
+    chg = (rho.mean() - rho).contiguous()
+    phi = torch.empty_like(rho)
+    for _ in range(2):
+        ctx.poisson(chg, run.E, phi)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        ctx.poisson(chg, run.E, phi)
+    b.record()
+    torch.cuda.synchronize()
+    field_ms = a.elapsed_time(b) / reps
+
+    # end to end through the public API with host buffers: pinned f0 -> device, K steps,
+    # device -> host of the final state and of the per-step energy/time/dt histories
+    host_f = torch.empty(run.f.shape, dtype=run.f.dtype, pin_memory=True)
+    host_f.copy_(run.f)
+    host_h = torch.empty((3, steps), dtype=torch.float64, pin_memory=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run.f.copy_(host_f, non_blocking=True)
+    g.replay()
+    host_f.copy_(run.f, non_blocking=True)
+    host_h.copy_(run.hist[:, :steps], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    dist.barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    state_bytes = run.f.numel() * es
+    del g
+    return {
+        "precision": precision, "ms": ms, "steps": steps, "dof": n_dof, "bytes_per_dof_step": 8 * es,
+        "stage_ms": stage_ms, "field_ms": field_ms, "e2e_ms": e2e_ms, "state_bytes": state_bytes,
+        "stage_bytes": [2 * es * n_dof, 3 * es * n_dof, 3 * es * n_dof],
+    }
+
+
+class _NoDist:
+    def barrier(self):
+        pass
+
+    def max(self, x):
+        return x
+
+    def sum(self, x):
+        return x
+
+
+class _TorchDist:
+    def __init__(self, torch, dist):
+        self.t = torch
+        self.d = dist
+
+    def barrier(self):
+        self.d.barrier()
+
+    def _reduce(self, x, op):
+        v = self.t.tensor([float(x)], dtype=self.t.float64, device="cuda")
+        self.d.all_reduce(v, op=op)
+        return float(v.item())
+
+    def max(self, x):
+        return self._reduce(x, self.d.ReduceOp.MAX)
+
+    def sum(self, x):
+        return self._reduce(x, self.d.ReduceOp.SUM)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # the reference's CPU path (oracle port, all host threads) on rank 0 only
+        if rank != 0:
+            return 0
+        rate, t, cores = cpu_port_rate(args.steps, args.warmup)
+        sample = (f"oracle (NumPy FP64 restatement of the reference step) on Nx={SAMPLE_RES[0]}, "
+                  f"Nu=Nv={SAMPLE_RES[1]}, n={ORDER}; {t:.2f} s/step")
+        line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "DOF-updates/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": "medium loss-cone config (Nx=32, Nu=Nv=50, n=8), CPU sample "
+                                       f"Nx={SAMPLE_RES[0]}", "dof_sample": dof(SAMPLE_RES, ORDER)},
+                "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": cores,
+                                 "kind": "port", "sample": sample},
+                "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = _TorchDist(torch, tdist)
+    else:
+        torch.cuda.set_device(0)
+        dist = _NoDist()
+
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    phys = int(vis.split(",")[local]) if vis and vis.split(",")[local].strip().isdigit() else local
+    results = {}
+    clocks = Clocks(phys)
+    with clocks:
+        for prec in ("fp64", "fp32"):
+            results[prec] = measure_precision(prec, args.steps, args.warmup, args.kernel_reps, dist)
+            torch.cuda.empty_cache()
+    ck = clocks.summary()
+
+    peak, peak_src = measured_peak_hbm()
+    out = {}
+    for prec, r in results.items():
+        ms_step = dist.max(r["ms"]) / r["steps"]
+        value = dist.sum(r["dof"] / (ms_step * 1e-3))
+        stage_s = sum(r["stage_ms"]) * 1e-3
+        achieved = sum(r["stage_bytes"]) / stage_s / 1e9
+        e2e_s = dist.max(r["e2e_ms"]) * 1e-3
+        out[prec] = {
+            "value": value, "ms_per_step": ms_step,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": f"stage_kernel<{ORDER},{'double' if prec == 'fp64' else 'float'}>",
+                         "algorithmic_bytes_per_dof_step": r["bytes_per_dof_step"],
+                         "stage_ms": r["stage_ms"], "field_ms": r["field_ms"],
+                         "step_effective_gbs": r["dof"] * r["bytes_per_dof_step"] / (ms_step * 1e-3) / 1e9,
+                         "peak_source": peak_src},
+            "e2e": {"value": dist.sum(r["dof"] * r["steps"] / e2e_s), "unit": "DOF-updates/s",
+                    "h2d_bytes_per_step": r["state_bytes"] / r["steps"],
+                    "d2h_bytes_per_step": (r["state_bytes"] + 24 * r["steps"]) / r["steps"]},
+        }
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    head = out["fp64"]
+    line = {
+        "metric": METRIC, "value": head["value"], "unit": "DOF-updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "medium loss-cone config: Nx=32, Nu=Nv=50, LGL n=8 "
+                               "(256x400x400 = 40.96M DOF per GPU), j=6, 1e-3 cos kx + 1e-6 noise, "
+                               "nonlinear SSP-RK3 + spectral Poisson per stage",
+                   "dof_per_gpu": dof(RES, ORDER), "l2": "inputs larger than L2 (377 MB FP64 state "
+                   "buffers, 3 buffers)", "parallelism": f"replicas x{world}"},
+        "roofline": head["roofline"],
+        "e2e": head["e2e"],
+        "gpu_launches": 6 * args.steps + 1,
+        "clocks": ck,
+        "variants": {"fp32_mixed": {"value": out["fp32"]["value"], "dtype": "f32",
+                                    "ms_per_step": out["fp32"]["ms_per_step"],
+                                    "roofline": out["fp32"]["roofline"], "e2e": out["fp32"]["e2e"],
+                                    "speedup_vs_fp64": out["fp32"]["value"] / head["value"]}},
+    }
+    if not args.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline_obj()
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,186 @@
+/*
+ * vlasov1d2v.h -- C ABI of the B200 (sm_100a) hot path of a 1D2V DG Vlasov-Poisson solver.
+ *
+ * Drop-in boundary for crewsdw/Vlasov1D2V's hot path: the semi-discrete DG right-hand side
+ * (main/fluxes.py), the SSP-RK3 loop (main/timestep.py), the zeroth velocity moment
+ * (main/grid.py) and the high-order-DFT Poisson solve (main/elliptic.py).  The reference
+ * binds these as Python classes over CuPy; the Python host layer of this project
+ * (vlasov1d2v_b200/) keeps those classes' signatures and calls the functions below through
+ * ctypes.
+ *
+ * Conventions
+ *   - Every state array is the reference's ghost-inclusive layout, C order:
+ *       f[X][n][U][n][V][n],  X = nx + 2, U = nu + 2, V = nv + 2
+ *     (main/grid.py:262-268).  Element index 0 and X-1 (U-1, V-1) are ghost elements.
+ *   - FP64 contexts take double* states, FP32 contexts take float* states (void* below).
+ *     Fields (E, phi, rho), energies and dt are always double.
+ *   - All pointers passed to compute entry points are DEVICE pointers unless the name says
+ *     host.  The library never allocates or frees caller buffers; it borrows them for the
+ *     duration of the call.  The context owns only its immutable coefficient tables.
+ *   - Work is enqueued on the caller's CUDA stream (cudaStream_t passed as void*; NULL =
+ *     legacy default stream).  Entry points do not synchronise the device, except
+ *     vl_ctx_create / vl_ctx_destroy (table upload / free).
+ *   - Every entry point returns an int status (VL_OK = 0; negative = error) and never
+ *     aborts the process.  vl_last_error() returns a message for the calling thread.
+ */
+#ifndef VLASOV1D2V_H
+#define VLASOV1D2V_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VL_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define VL_API __attribute__((visibility("default")))
+#else
+#define VL_API
+#endif
+
+enum vl_status {
+    VL_OK = 0,
+    VL_ERR_INVALID = -1,     /* bad shape, order, null pointer or argument */
+    VL_ERR_CUDA = -2,        /* a CUDA runtime call failed (message in vl_last_error) */
+    VL_ERR_NONFINITE = -3,   /* a non-finite density / field / energy was detected */
+    VL_ERR_UNSUPPORTED = -4, /* order or precision not compiled in */
+    VL_ERR_TOO_LARGE = -5    /* a size exceeds a fixed capacity of the entry point */
+};
+
+enum vl_precision { VL_FP64 = 0, VL_FP32 = 1 };
+
+/* x-halo convention of the RHS (main/fluxes.py:164-174 rolls over the ghost-inclusive axis):
+ *   VL_XHALO_GHOST    read the x-ghost slabs of the input (reference semantics for a raw
+ *                     semi_discrete_rhs call on an arbitrary array);
+ *   VL_XHALO_PERIODIC wrap to the opposite interior slab (what the stepper's ghost sync,
+ *                     main/timestep.py:143 and :167-168, makes equivalent).               */
+enum vl_xhalo { VL_XHALO_GHOST = 0, VL_XHALO_PERIODIC = 1 };
+
+/* Problem description.  Host pointers; copied into the context by vl_ctx_create. */
+typedef struct vl_config {
+    int32_t abi_version;      /* = VL_ABI_VERSION */
+    int32_t precision;        /* enum vl_precision */
+    int32_t nx, nu, nv;       /* interior element counts (Grid1D.res, main/grid.py:14) */
+    int32_t n;                /* LGL nodes per element, 1..10 (Basis1D.order) */
+    int32_t n_modes;          /* M = number of DFT wave numbers (main/grid.py:46-48) */
+    int32_t reserved0;
+    double accel;             /* electron acceleration multiplier (main/reference.py:61) */
+    double bfield;            /* magnetic field B (Elliptic.magnetic_field) */
+    double kappa;             /* Poisson coefficient (main/reference.py:63) */
+    double jx, ju, jv;        /* element Jacobians 2/dx (main/grid.py:23) */
+    double dx, du, dv;        /* element widths (main/grid.py:20) */
+    double length_x;          /* x-domain length L (main/grid.py:19) */
+    double umax, vmax;        /* max |node coordinate| incl. ghosts (main/grid.py:32) */
+    double courant;           /* Courant number (main/timestep.py:78-79) */
+    const double *up;         /* [n][n]   internal-flux matrix (main/basis.py:176-188) */
+    const double *xi;         /* [n][2]   lift columns of the inverse mass (main/basis.py:110) */
+    const double *xw;         /* [n]      LGL weights (Grid1D.quad_weights row, main/grid.py:26) */
+    const double *u_nodes;    /* [(nu+2)*n] ghost-inclusive u coordinates (Grid1D.arr) */
+    const double *v_nodes;    /* [(nv+2)*n] ghost-inclusive v coordinates */
+    const double *wave_numbers; /* [M] */
+    const double *dft_fwd;    /* [nx][n][M] complex, interleaved re/im (Grid1D.spectral_transform) */
+    const double *dft_inv;    /* [M][nx][n] complex, interleaved re/im (Grid1D.grid_phases) */
+} vl_config;
+
+typedef struct vl_ctx vl_ctx;
+
+/* Device-resident loop state of the SSP-RK3 driver (Stepper.main_loop, main/timestep.py:81-139).
+ * The caller allocates it (device memory, 64-byte aligned) and initialises it with
+ * vl_run_state_init.  Kernels read and update it, so the loop runs without host syncs.     */
+typedef struct vl_run_state {
+    double dt;          /* dt of the running step (Stepper.dt) */
+    double dt_next;     /* dt computed after stage 2 (main/timestep.py:184-185) */
+    double time;        /* Stepper.time; advanced by the NEW dt after each step (ts:98) */
+    double final_time;  /* the loop ends once time >= final_time (ts:91) */
+    int64_t steps;      /* Stepper.steps_counter */
+    int64_t max_steps;  /* the loop also ends once steps >= max_steps */
+    int32_t active;     /* the step in flight runs (set at its first kernel) */
+    int32_t active_next;/* whether the next step runs */
+    int32_t status;     /* 0 ok; bit 0: non-finite density/field/energy */
+    int32_t hist_capacity; /* ring size of the history arrays */
+    double *energy_hist;/* [hist_capacity] field energy after step s at [s % cap] (ts:102-103) */
+    double *time_hist;  /* [hist_capacity] time after step s */
+    double *dt_hist;    /* [hist_capacity] dt after step s */
+    double reserved[4];
+} vl_run_state;
+
+/* ---- context ------------------------------------------------------------------------- */
+VL_API int vl_ctx_create(const vl_config *cfg, vl_ctx **out);
+VL_API int vl_ctx_destroy(vl_ctx *ctx);
+VL_API const char *vl_last_error(void);
+VL_API int vl_abi_version(void);
+
+/* number of elements of one ghost-inclusive state array: (nx+2) n (nu+2) n (nv+2) n */
+VL_API size_t vl_state_elems(const vl_ctx *ctx);
+/* bytes of scratch the stepper / moment entry points need (caller allocates, 256-B aligned) */
+VL_API size_t vl_workspace_bytes(const vl_ctx *ctx);
+
+/* ---- hot-path operators ------------------------------------------------------------------ */
+
+/* DGFlux.semi_discrete_rhs (main/fluxes.py:59-105): out[interior] = J_x F_x + J_u F_u + J_v F_v
+ * for the ghost-inclusive state f with field E[(nx+2)][n] (main/elliptic.py:132-145).
+ * Ghost rows of out are not written (the reference discards them).                        */
+VL_API int vl_rhs(vl_ctx *ctx, const void *f, const double *E, void *out, int xhalo, void *stream);
+
+/* The same operator with caller-chosen direction weights: out = w[0] F_x + w[1] F_u + w[2] F_v.
+ * w = {1, 0, 0}, {0, 1, 0}, {0, 0, 1} give DGFlux.x_flux / u_flux / v_flux (main/fluxes.py:107-153),
+ * which return the flux divergence of one direction without its Jacobian.                  */
+VL_API int vl_rhs_weighted(vl_ctx *ctx, const void *f, const double *E, void *out, int xhalo,
+                    const double *w_host, void *stream);
+
+/* Distribution.moment_zero / moment_zero_of_arr (main/grid.py:303-321):
+ * rho[nx][n] = sum over interior velocity nodes of f w_u w_v / (J_u J_v).                   */
+VL_API int vl_moment(vl_ctx *ctx, const void *f, double *rho, void *stream);
+
+/* Elliptic.poisson2 (main/elliptic.py:117-145): spectral solve of the charge density
+ * (already mean-subtracted by the caller, as main/timestep.py:155 does).  Writes
+ * E[(nx+2)][n] (ghosts periodic) and phi[nx][n] (phi may be NULL).                        */
+VL_API int vl_poisson(vl_ctx *ctx, const double *charge_density, double *E, double *phi,
+               void *stream);
+
+/* Elliptic.electric_energy (main/elliptic.py:150-151): 0.5 sum_i w_i E[1:-1]^2 -> *energy. */
+VL_API int vl_field_energy(vl_ctx *ctx, const double *E, double *energy, void *stream);
+
+/* get_max_speeds + Stepper.adapt_time_step (main/timestep.py:231-242) from E -> *dt.       */
+VL_API int vl_adapt_dt(vl_ctx *ctx, const double *E, double *dt, void *stream);
+
+/* One fused SSP-RK stage (main/timestep.py:157-163 and :174-182):
+ *   stage 0:  out = in + dt * RHS(in)                       (in is f^n)
+ *   stage 1:  out = 3/4 fn + 1/4 in + 1/4 dt RHS(in)
+ *   stage 2:  out = 1/3 fn + 2/3 in + 2/3 dt RHS(in)
+ * dt is read from device memory (*dt).  Interior of out only.  If rho_partials is not NULL
+ * the stage also writes the moment partials of out (consumed by vl_poisson_from_partials). */
+VL_API int vl_rk_stage(vl_ctx *ctx, int stage, const void *in, const void *fn, void *out,
+                const double *E, const double *dt, int xhalo, void *workspace, void *stream);
+
+/* ---- the loop ------------------------------------------------------------------------------ */
+
+/* Fill a device vl_run_state: dt from E0 (adapt rule), time 0, steps 0, histories given.
+ * E0 is the field solved before the loop (main/main.py:131); its energy is returned in
+ * *energy0 (device pointer, may be NULL).                                                    */
+VL_API int vl_run_state_init(vl_ctx *ctx, vl_run_state *state, const double *E0, double final_time,
+                      int64_t max_steps, double *energy_hist, double *time_hist,
+                      double *dt_hist, int32_t hist_capacity, double *energy0, void *stream);
+
+/* Stepper.nonlinear_ssp_rk x nsteps (main/timestep.py:141-187) with the main loop's
+ * bookkeeping (ts:91-103), entirely on the device: each step runs only while
+ * state->time < final_time and steps < max_steps (checked on the device, so extra steps
+ * in a batch are no-ops).  f is advanced in place.  stage_a / stage_b are state-sized
+ * buffers whose velocity-ghost elements must equal f's (vl_sync_ghosts does that).
+ * E / phi receive the last field solved (of RK stage s1, as in the reference).             */
+VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, double *E,
+                     double *phi, vl_run_state *state, void *workspace, int nsteps,
+                     void *stream);
+
+/* Copy f's ghost elements (all six ghost slabs) into a stage buffer and perform the
+ * reference's periodic x-ghost swap on f (Distribution.swap_ghost_cells_of_array,
+ * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */
+VL_API int vl_sync_ghosts(vl_ctx *ctx, void *f, void *stage, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VLASOV1D2V_H */

@@ -1,0 +1,93 @@
+"""Pin the CPU oracle against fixtures generated by the reference itself (tests/golden).
+
+The fixtures come from ``tests/golden/make_golden.py``, which runs crewsdw/Vlasov1D2V's own
+modules on the CPU.  These tests need no GPU.
+"""
+import numpy as np
+import pytest
+
+from helpers import INNER, SMALL_CASES, case_setup, field_rtol, golden, rel_err
+from oracle import vlasov_oracle as vo
+
+
+def test_basis_tables():
+    """The oracle computes LGL constants in extended precision (correctly rounded); the
+    reference evaluates sqrt(1/5), sqrt(3/7), ... in double for n <= 6, so nodes may differ by
+    an ulp there.  Matrices agree to 1e-13."""
+    g = golden("basis")
+    for n in range(1, 11):
+        b = vo.make_basis(n)
+        np.testing.assert_allclose(b.nodes, g[f"n{n}_nodes"], rtol=0, atol=2.3e-16)
+        np.testing.assert_allclose(b.weights, g[f"n{n}_weights"], rtol=5e-16, atol=0)
+        for key, mine in (("vinv", b.vinv), ("invm", b.invm), ("up", b.up), ("xi", b.xi)):
+            ref = g[f"n{n}_{key}"]
+            assert np.max(np.abs(mine - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref))), (n, key)
+    np.testing.assert_array_equal(vo.COURANT_RK3, g["courant_rk3"])
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_grid_and_dft_tables(name):
+    G, res, n = case_setup(name)
+    c = vo.make_case(*res, n)
+    np.testing.assert_array_equal(c.x.arr, G["x_arr"])
+    np.testing.assert_array_equal(c.u.arr, G["u_arr"])
+    np.testing.assert_array_equal(c.v.arr, G["v_arr"])
+    np.testing.assert_array_equal(c.x.wave_numbers, G["wave_numbers"])
+    np.testing.assert_array_equal(c.x.T, G["T"])
+    np.testing.assert_array_equal(c.x.P, G["P"])
+    assert c.accel == G["accel"] and c.kappa == G["kappa"] and c.B == G["B"]
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_rhs(name):
+    G, res, n = case_setup(name)
+    c = vo.make_case(*res, n)
+    assert rel_err(vo.rhs(G["f_init"], G["E_init"], c)[INNER], G["rhs_init"]) < 1e-12
+    assert rel_err(vo.rhs(G["f_rand"], G["E_rand"], c)[INNER], G["rhs_rand"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_moment_poisson_energy(name):
+    G, res, n = case_setup(name)
+    c = vo.make_case(*res, n)
+    rho = vo.moment_zero(G["f_rand"], c)
+    assert rel_err(rho, G["rho_rand"]) < 1e-14
+    E, phi = vo.poisson2(np.mean(rho) - rho, c)
+    tol = field_rtol(G["rho_rand"])
+    assert rel_err(E, G["E_rand_solved"]) < tol
+    assert rel_err(phi, G["phi_rand_solved"]) < tol
+    assert abs(vo.electric_energy(E, c) / G["energy_rand_solved"] - 1) < 2 * tol
+    rho0 = vo.moment_zero(G["f_init"], c)
+    assert rel_err(rho0, G["rho_init"]) < 1e-14
+    E0, _ = vo.poisson2(rho0 - np.mean(rho0), c)
+    assert rel_err(E0, G["E_init"]) < field_rtol(G["rho_init"])
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+def test_steps(name):
+    G, res, n = case_setup(name)
+    c = vo.make_case(*res, n)
+    f = G["f_init"].copy()
+    nst = len(G["energy"]) - 1
+    rho0 = vo.moment_zero(f, c)
+    E0, _ = vo.poisson2(rho0 - np.mean(rho0), c)
+    rec = vo.run(f, c, steps=nst, E0=E0)
+    tol = field_rtol(G["rho_init"])
+    np.testing.assert_allclose(rec.field_energy, G["energy"], rtol=2 * tol, atol=0)
+    np.testing.assert_allclose(rec.dt_history, G["dt"], rtol=1e-14, atol=0)
+    np.testing.assert_allclose(rec.time_array, G["time"], rtol=1e-14, atol=0)
+    assert rel_err(f[INNER], G[f"f_step{nst}"]) < 1e-12
+
+
+def test_cfg1_first_steps():
+    """Config 1 (16^3 elements, n = 8, 1 + 0.01 cos kx): three oracle steps against the first
+    entries of the reference's 200-step histories."""
+    G = golden("cfg1_200")
+    c = vo.make_case(16, 16, 16, 8)
+    f = vo.cos_perturbed(c, c.extra["norm"].vt_e, 6, 0.01)
+    assert f.sum() == G["f_init_sum"]
+    np.testing.assert_array_equal(f[5, 3, 7, 2, 9, 4:8], G["f_init_probe"])
+    rec = vo.run(f, c, steps=3)
+    np.testing.assert_allclose(rec.field_energy, G["energy"][:4], rtol=1e-12)
+    np.testing.assert_allclose(rec.dt_history, G["dt"][:4], rtol=1e-14)
+    np.testing.assert_allclose(rec.time_array, G["time"][:4], rtol=1e-14)

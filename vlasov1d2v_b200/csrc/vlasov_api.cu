@@ -1,0 +1,543 @@
+// C ABI of the B200 hot path (declarations and reference citations in include/vlasov1d2v.h).
+//
+// Ownership: the context holds the immutable coefficient tables (device copies of the node
+// coordinates and DFT tensors, host copies of the small matrices that travel as kernel
+// parameters).  State, field, workspace and loop-state buffers belong to the caller.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "vlasov1d2v.h"
+#include "vlasov_kernels.cuh"
+
+struct vl_ctx {
+    vl_config cfg;      // scalars (pointer members cleared)
+    int device;
+    int sm_count;
+    int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
+    double up[vl::NMAX * vl::NMAX];
+    double xi[vl::NMAX * 2];
+    double xw[vl::NMAX];
+    double qw[vl::NMAX * vl::NMAX];
+    double *d_unodes = nullptr;
+    double *d_vnodes = nullptr;
+    double *d_k = nullptr;
+    double *d_xw = nullptr;
+    double2 *d_fwd = nullptr;
+    double2 *d_inv = nullptr;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return VL_ERR_CUDA;
+}
+
+#define VL_CUDA(call)                                              \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);        \
+    } while (0)
+
+inline int check_launch(const char *where) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, where);
+    return VL_OK;
+}
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+inline size_t elem_size(const vl_ctx *c) {
+    return c->cfg.precision == VL_FP64 ? sizeof(double) : sizeof(float);
+}
+
+// ------------------------------------------------------------------------------------------
+// stage kernel dispatch
+// ------------------------------------------------------------------------------------------
+template <int N, typename T>
+int launch_stage_t(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
+    using G = vl::StageGeom<N>;
+    vl::StageTables<T> tb;
+    std::memset(&tb, 0, sizeof(tb));
+    for (int i = 0; i < N * N; ++i) tb.up[i] = (T)c->up[i];
+    for (int i = 0; i < 2 * N; ++i) tb.xi[i] = (T)c->xi[i];
+    for (int i = 0; i < N * N; ++i) tb.qw[i] = c->qw[i];
+    const size_t smem = G::template smem_bytes<T>();
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaFuncSetAttribute(vl::stage_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        attr_done = true;
+    }
+    dim3 grid(c->stage_grid_g, c->cfg.nx);
+    vl::stage_kernel<N, T><<<grid, vl::STAGE_THREADS, smem, s>>>(a, tb);
+    return check_launch("stage_kernel");
+}
+
+template <typename T>
+int launch_stage(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
+    switch (c->cfg.n) {
+        case 1: return launch_stage_t<1, T>(c, a, s);
+        case 2: return launch_stage_t<2, T>(c, a, s);
+        case 3: return launch_stage_t<3, T>(c, a, s);
+        case 4: return launch_stage_t<4, T>(c, a, s);
+        case 5: return launch_stage_t<5, T>(c, a, s);
+        case 6: return launch_stage_t<6, T>(c, a, s);
+        case 7: return launch_stage_t<7, T>(c, a, s);
+        case 8: return launch_stage_t<8, T>(c, a, s);
+        case 9: return launch_stage_t<9, T>(c, a, s);
+        case 10: return launch_stage_t<10, T>(c, a, s);
+        default: return fail(VL_ERR_UNSUPPORTED, "order n not compiled in");
+    }
+}
+
+int stage(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
+    return c->cfg.precision == VL_FP64 ? launch_stage<double>(c, a, s)
+                                       : launch_stage<float>(c, a, s);
+}
+
+template <int N, typename T>
+int stage_occupancy_t() {
+    using G = vl::StageGeom<N>;
+    int blocks = 0;
+    const size_t smem = G::template smem_bytes<T>();
+    cudaFuncSetAttribute(vl::stage_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_kernel<N, T>,
+                                                      vl::STAGE_THREADS, smem) != cudaSuccess)
+        return 1;
+    return blocks > 0 ? blocks : 1;
+}
+
+template <typename T>
+int stage_occupancy(int n) {
+    switch (n) {
+        case 1: return stage_occupancy_t<1, T>();
+        case 2: return stage_occupancy_t<2, T>();
+        case 3: return stage_occupancy_t<3, T>();
+        case 4: return stage_occupancy_t<4, T>();
+        case 5: return stage_occupancy_t<5, T>();
+        case 6: return stage_occupancy_t<6, T>();
+        case 7: return stage_occupancy_t<7, T>();
+        case 8: return stage_occupancy_t<8, T>();
+        case 9: return stage_occupancy_t<9, T>();
+        case 10: return stage_occupancy_t<10, T>();
+        default: return 1;
+    }
+}
+
+int stage_bt(int n) {
+    switch (n) {
+        case 1: return vl::StageGeom<1>::BT;
+        case 2: return vl::StageGeom<2>::BT;
+        case 3: return vl::StageGeom<3>::BT;
+        case 4: return vl::StageGeom<4>::BT;
+        case 5: return vl::StageGeom<5>::BT;
+        case 6: return vl::StageGeom<6>::BT;
+        case 7: return vl::StageGeom<7>::BT;
+        case 8: return vl::StageGeom<8>::BT;
+        case 9: return vl::StageGeom<9>::BT;
+        default: return vl::StageGeom<10>::BT;
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// moment kernel dispatch
+// ------------------------------------------------------------------------------------------
+template <int N, typename T>
+int launch_moment_t(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s) {
+    vl::MomentArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.f = f;
+    a.out = out;
+    a.G = G;
+    a.nx = c->cfg.nx;
+    a.nu = c->cfg.nu;
+    a.nv = c->cfg.nv;
+    for (int i = 0; i < N * N; ++i) a.qw[i] = c->qw[i];
+    vl::moment_kernel<N, T><<<c->cfg.nx * N, 256, 0, s>>>(a);
+    return check_launch("moment_kernel");
+}
+
+template <typename T>
+int launch_moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s) {
+    switch (c->cfg.n) {
+        case 1: return launch_moment_t<1, T>(c, f, out, G, s);
+        case 2: return launch_moment_t<2, T>(c, f, out, G, s);
+        case 3: return launch_moment_t<3, T>(c, f, out, G, s);
+        case 4: return launch_moment_t<4, T>(c, f, out, G, s);
+        case 5: return launch_moment_t<5, T>(c, f, out, G, s);
+        case 6: return launch_moment_t<6, T>(c, f, out, G, s);
+        case 7: return launch_moment_t<7, T>(c, f, out, G, s);
+        case 8: return launch_moment_t<8, T>(c, f, out, G, s);
+        case 9: return launch_moment_t<9, T>(c, f, out, G, s);
+        case 10: return launch_moment_t<10, T>(c, f, out, G, s);
+        default: return fail(VL_ERR_UNSUPPORTED, "order n not compiled in");
+    }
+}
+
+int moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s) {
+    return c->cfg.precision == VL_FP64 ? launch_moment<double>(c, f, out, G, s)
+                                       : launch_moment<float>(c, f, out, G, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// field / scalar kernels
+// ------------------------------------------------------------------------------------------
+vl::FieldArgs field_args(const vl_ctx *c) {
+    vl::FieldArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.fwd = c->d_fwd;
+    a.inv = c->d_inv;
+    a.k = c->d_k;
+    a.xw = c->d_xw;
+    a.nx = c->cfg.nx;
+    a.n = c->cfg.n;
+    a.M = c->cfg.n_modes;
+    a.kappa = c->cfg.kappa;
+    a.dx = c->cfg.dx;
+    a.length = c->cfg.length_x;
+    a.accel = c->cfg.accel;
+    a.bfield = c->cfg.bfield;
+    a.umax = c->cfg.umax;
+    a.vmax = c->cfg.vmax;
+    a.du = c->cfg.du;
+    a.dv = c->cfg.dv;
+    a.courant = c->cfg.courant;
+    return a;
+}
+
+int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
+    vl::field_kernel<<<1, vl::FIELD_THREADS, 0, s>>>(a);
+    return check_launch("field_kernel");
+}
+
+vl::ScalarArgs scalar_args(const vl_ctx *c, const double *E) {
+    vl::ScalarArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.E = E;
+    a.xw = c->d_xw;
+    a.nx = c->cfg.nx;
+    a.n = c->cfg.n;
+    a.accel = c->cfg.accel;
+    a.bfield = c->cfg.bfield;
+    a.umax = c->cfg.umax;
+    a.vmax = c->cfg.vmax;
+    a.dx = c->cfg.dx;
+    a.du = c->cfg.du;
+    a.dv = c->cfg.dv;
+    a.courant = c->cfg.courant;
+    return a;
+}
+
+vl::StageArgs stage_args(const vl_ctx *c) {
+    vl::StageArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.u_nodes = c->d_unodes;
+    a.v_nodes = c->d_vnodes;
+    a.nx = c->cfg.nx;
+    a.nu = c->cfg.nu;
+    a.nv = c->cfg.nv;
+    a.accel = c->cfg.accel;
+    a.bfield = c->cfg.bfield;
+    a.jx = c->cfg.jx;
+    a.ju = c->cfg.ju;
+    a.jv = c->cfg.jv;
+    return a;
+}
+
+// Shu-Osher coefficients of the nonlinear SSP-RK3 (main/timestep.py:35-39)
+const double kRK3[2][3] = {{3.0 / 4.0, 1.0 / 4.0, 1.0 / 4.0}, {1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0}};
+
+template <typename P>
+int upload(P **dst, const void *src, size_t bytes) {
+    VL_CUDA(cudaMalloc((void **)dst, bytes));
+    VL_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+    return VL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *vl_last_error(void) { return g_err.c_str(); }
+
+int vl_abi_version(void) { return VL_ABI_VERSION; }
+
+int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
+    if (cfg == nullptr || out == nullptr) return fail(VL_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (cfg->abi_version != VL_ABI_VERSION) return fail(VL_ERR_INVALID, "ABI version mismatch");
+    if (cfg->precision != VL_FP64 && cfg->precision != VL_FP32)
+        return fail(VL_ERR_INVALID, "precision must be VL_FP64 or VL_FP32");
+    if (cfg->n < 1 || cfg->n > vl::NMAX) return fail(VL_ERR_UNSUPPORTED, "n must be in 1..10");
+    if (cfg->nx < 1 || cfg->nu < 1 || cfg->nv < 1) return fail(VL_ERR_INVALID, "empty grid");
+    if (cfg->nx * cfg->n > vl::FIELD_MAX_NODES)
+        return fail(VL_ERR_TOO_LARGE, "nx * n exceeds the field kernel capacity (640)");
+    if (cfg->n_modes < 1 || cfg->n_modes > vl::FIELD_MAX_MODES)
+        return fail(VL_ERR_TOO_LARGE, "number of DFT modes exceeds the field kernel capacity (321)");
+    if (!cfg->up || !cfg->xi || !cfg->xw || !cfg->u_nodes || !cfg->v_nodes || !cfg->wave_numbers ||
+        !cfg->dft_fwd || !cfg->dft_inv)
+        return fail(VL_ERR_INVALID, "null table pointer");
+    const size_t elems = (size_t)(cfg->nx + 2) * cfg->n * (cfg->nu + 2) * cfg->n *
+                         (cfg->nv + 2) * cfg->n;
+    if (elems >= ((size_t)1 << 40)) return fail(VL_ERR_TOO_LARGE, "state too large");
+
+    vl_ctx *c = new vl_ctx();
+    c->cfg = *cfg;
+    c->cfg.up = c->cfg.xi = c->cfg.xw = c->cfg.u_nodes = c->cfg.v_nodes = nullptr;
+    c->cfg.wave_numbers = c->cfg.dft_fwd = c->cfg.dft_inv = nullptr;
+    const int n = cfg->n;
+    std::memset(c->up, 0, sizeof(c->up));
+    std::memset(c->xi, 0, sizeof(c->xi));
+    std::memset(c->qw, 0, sizeof(c->qw));
+    std::memcpy(c->up, cfg->up, sizeof(double) * n * n);
+    std::memcpy(c->xi, cfg->xi, sizeof(double) * n * 2);
+    std::memcpy(c->xw, cfg->xw, sizeof(double) * n);
+    // velocity quadrature weights w_j w_k / (J_u J_v) (main/grid.py:297-301)
+    const double jj = cfg->ju * cfg->jv;
+    for (int j = 0; j < n; ++j)
+        for (int k = 0; k < n; ++k) c->qw[j * n + k] = (cfg->xw[j] * cfg->xw[k]) / jj;
+
+    int rc = VL_OK;
+    auto cleanup = [&](int code) {
+        vl_ctx_destroy(c);
+        return code;
+    };
+    cudaError_t e = cudaGetDevice(&c->device);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaGetDevice"));
+    e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaDeviceGetAttribute"));
+    if ((rc = upload(&c->d_unodes, cfg->u_nodes, sizeof(double) * (cfg->nu + 2) * n))) return cleanup(rc);
+    if ((rc = upload(&c->d_vnodes, cfg->v_nodes, sizeof(double) * (cfg->nv + 2) * n))) return cleanup(rc);
+    if ((rc = upload(&c->d_k, cfg->wave_numbers, sizeof(double) * cfg->n_modes))) return cleanup(rc);
+    if ((rc = upload(&c->d_xw, cfg->xw, sizeof(double) * n))) return cleanup(rc);
+    const size_t tbytes = sizeof(double2) * (size_t)cfg->nx * n * cfg->n_modes;
+    if ((rc = upload(&c->d_fwd, cfg->dft_fwd, tbytes))) return cleanup(rc);
+    if ((rc = upload(&c->d_inv, cfg->dft_inv, tbytes))) return cleanup(rc);
+
+    // CTAs per x element: fill the device (resident CTAs x SMs), at most one per tile
+    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n) : stage_occupancy<float>(n);
+    const int bt = stage_bt(n);
+    const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
+    int g = (c->sm_count * occ + cfg->nx - 1) / cfg->nx;
+    if (g > tiles) g = tiles;
+    if (g < 1) g = 1;
+    c->stage_grid_g = g;
+    *out = c;
+    return VL_OK;
+}
+
+int vl_ctx_destroy(vl_ctx *c) {
+    if (c == nullptr) return VL_OK;
+    cudaFree(c->d_unodes);
+    cudaFree(c->d_vnodes);
+    cudaFree(c->d_k);
+    cudaFree(c->d_xw);
+    cudaFree(c->d_fwd);
+    cudaFree(c->d_inv);
+    delete c;
+    return VL_OK;
+}
+
+size_t vl_state_elems(const vl_ctx *c) {
+    if (c == nullptr) return 0;
+    const vl_config &g = c->cfg;
+    return (size_t)(g.nx + 2) * g.n * (g.nu + 2) * g.n * (g.nv + 2) * g.n;
+}
+
+size_t vl_workspace_bytes(const vl_ctx *c) {
+    if (c == nullptr) return 0;
+    const size_t b = sizeof(double) * (size_t)c->cfg.nx * c->stage_grid_g * c->cfg.n;
+    return (b + 255) & ~(size_t)255;
+}
+
+int vl_rhs(vl_ctx *c, const void *f, const double *E, void *out, int xhalo, void *stream) {
+    if (!c || !f || !E || !out) return fail(VL_ERR_INVALID, "null argument");
+    if (xhalo != VL_XHALO_GHOST && xhalo != VL_XHALO_PERIODIC) return fail(VL_ERR_INVALID, "xhalo");
+    vl::StageArgs a = stage_args(c);
+    a.in = f;
+    a.out = out;
+    a.E = E;
+    a.xhalo = xhalo;
+    a.kind = vl::KIND_RHS;
+    return stage(c, a, as_stream(stream));
+}
+
+int vl_rhs_weighted(vl_ctx *c, const void *f, const double *E, void *out, int xhalo,
+                    const double *w, void *stream) {
+    if (!c || !f || !E || !out || !w) return fail(VL_ERR_INVALID, "null argument");
+    if (xhalo != VL_XHALO_GHOST && xhalo != VL_XHALO_PERIODIC) return fail(VL_ERR_INVALID, "xhalo");
+    vl::StageArgs a = stage_args(c);
+    a.in = f;
+    a.out = out;
+    a.E = E;
+    a.xhalo = xhalo;
+    a.kind = vl::KIND_RHS;
+    a.jx = w[0];
+    a.ju = w[1];
+    a.jv = w[2];
+    return stage(c, a, as_stream(stream));
+}
+
+int vl_moment(vl_ctx *c, const void *f, double *rho, void *stream) {
+    if (!c || !f || !rho) return fail(VL_ERR_INVALID, "null argument");
+    return moment(c, f, rho, 1, as_stream(stream));
+}
+
+int vl_poisson(vl_ctx *c, const double *charge, double *E, double *phi, void *stream) {
+    if (!c || !charge || !E) return fail(VL_ERR_INVALID, "null argument");
+    vl::FieldArgs a = field_args(c);
+    a.charge_in = charge;
+    a.E = E;
+    a.phi = phi;
+    return field(c, a, as_stream(stream));
+}
+
+int vl_field_energy(vl_ctx *c, const double *E, double *energy, void *stream) {
+    if (!c || !E || !energy) return fail(VL_ERR_INVALID, "null argument");
+    vl::ScalarArgs a = scalar_args(c, E);
+    a.energy = energy;
+    vl::scalars_kernel<<<1, vl::FIELD_THREADS, 0, as_stream(stream)>>>(a);
+    return check_launch("scalars_kernel");
+}
+
+int vl_adapt_dt(vl_ctx *c, const double *E, double *dt, void *stream) {
+    if (!c || !E || !dt) return fail(VL_ERR_INVALID, "null argument");
+    vl::ScalarArgs a = scalar_args(c, E);
+    a.dt = dt;
+    vl::scalars_kernel<<<1, vl::FIELD_THREADS, 0, as_stream(stream)>>>(a);
+    return check_launch("scalars_kernel");
+}
+
+int vl_rk_stage(vl_ctx *c, int stg, const void *in, const void *fn, void *out, const double *E,
+                const double *dt, int xhalo, void *workspace, void *stream) {
+    if (!c || !in || !out || !E || !dt) return fail(VL_ERR_INVALID, "null argument");
+    if (stg < 0 || stg > 2) return fail(VL_ERR_INVALID, "stage must be 0, 1 or 2");
+    if (stg > 0 && !fn) return fail(VL_ERR_INVALID, "fn required for stages 1 and 2");
+    if (xhalo != VL_XHALO_GHOST && xhalo != VL_XHALO_PERIODIC) return fail(VL_ERR_INVALID, "xhalo");
+    vl::StageArgs a = stage_args(c);
+    a.in = in;
+    a.fn = fn;
+    a.out = out;
+    a.E = E;
+    a.dt = dt;
+    a.xhalo = xhalo;
+    a.partials = static_cast<double *>(workspace);
+    if (stg == 0) {
+        a.kind = vl::KIND_EULER;
+    } else {
+        a.kind = vl::KIND_COMBINE;
+        a.c0 = kRK3[stg - 1][0];
+        a.c1 = kRK3[stg - 1][1];
+        a.c2 = kRK3[stg - 1][2];
+    }
+    return stage(c, a, as_stream(stream));
+}
+
+int vl_run_state_init(vl_ctx *c, vl_run_state *state, const double *E0, double final_time,
+                      int64_t max_steps, double *eh, double *th, double *dh, int32_t cap,
+                      double *energy0, void *stream) {
+    if (!c || !state || !E0) return fail(VL_ERR_INVALID, "null argument");
+    if (cap < 0) return fail(VL_ERR_INVALID, "history capacity");
+    vl::ScalarArgs a = scalar_args(c, E0);
+    a.energy = energy0;
+    a.init = state;
+    a.final_time = final_time;
+    a.max_steps = max_steps;
+    a.eh = eh;
+    a.th = th;
+    a.dh = dh;
+    a.cap = cap;
+    vl::scalars_kernel<<<1, vl::FIELD_THREADS, 0, as_stream(stream)>>>(a);
+    return check_launch("scalars_kernel(init)");
+}
+
+int vl_sync_ghosts(vl_ctx *c, void *f, void *stage_buf, void *stream) {
+    if (!c || !f) return fail(VL_ERR_INVALID, "null argument");
+    cudaStream_t s = as_stream(stream);
+    const size_t es = elem_size(c);
+    const size_t slab = vl_state_elems(c) / (size_t)(c->cfg.nx + 2) * es;
+    char *fb = static_cast<char *>(f);
+    // Distribution.swap_ghost_cells_of_array (main/grid.py:187-189)
+    VL_CUDA(cudaMemcpyAsync(fb, fb + slab * c->cfg.nx, slab, cudaMemcpyDeviceToDevice, s));
+    VL_CUDA(cudaMemcpyAsync(fb + slab * (c->cfg.nx + 1), fb + slab, slab, cudaMemcpyDeviceToDevice, s));
+    if (stage_buf != nullptr && stage_buf != f)
+        VL_CUDA(cudaMemcpyAsync(stage_buf, f, vl_state_elems(c) * es, cudaMemcpyDeviceToDevice, s));
+    return VL_OK;
+}
+
+int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *phi,
+                     vl_run_state *state, void *workspace, int nsteps, void *stream) {
+    if (!c || !f || !sa || !sb || !E || !state || !workspace)
+        return fail(VL_ERR_INVALID, "null argument");
+    if (nsteps < 0) return fail(VL_ERR_INVALID, "nsteps < 0");
+    cudaStream_t s = as_stream(stream);
+    double *partials = static_cast<double *>(workspace);
+    const int G = c->stage_grid_g;
+    int rc;
+    // moment partials of f^n for the first step's field solve
+    if ((rc = moment(c, f, partials, G, s))) return rc;
+    vl::FieldArgs fa = field_args(c);
+    fa.partials = partials;
+    fa.G = G;
+    fa.E = E;
+    fa.state = state;
+    vl::StageArgs st = stage_args(c);
+    st.E = E;
+    st.dt = &state->dt;
+    st.state = state;
+    st.xhalo = VL_XHALO_PERIODIC;
+    st.partials = partials;
+    for (int it = 0; it < nsteps; ++it) {
+        // stage 0: E(f^n); s0 = f + dt R(f)  (main/timestep.py:153-163)
+        fa.mode = vl::FIELD_PROMOTE;
+        fa.phi = nullptr;
+        if ((rc = field(c, fa, s))) return rc;
+        st.in = f;
+        st.fn = nullptr;
+        st.out = sa;
+        st.ghost_out = f;
+        st.kind = vl::KIND_EULER;
+        if ((rc = stage(c, st, s))) return rc;
+        // stage 1: E(s0); s1 = 3/4 f + 1/4 s0 + 1/4 dt R(s0)
+        fa.mode = vl::FIELD_REQUIRE_ACTIVE;
+        if ((rc = field(c, fa, s))) return rc;
+        st.in = sa;
+        st.fn = f;
+        st.out = sb;
+        st.ghost_out = nullptr;
+        st.kind = vl::KIND_COMBINE;
+        st.c0 = kRK3[0][0];
+        st.c1 = kRK3[0][1];
+        st.c2 = kRK3[0][2];
+        if ((rc = stage(c, st, s))) return rc;
+        // stage 2: E(s1) (+ energy, dt, time: main/timestep.py:98-103, :184-185);
+        //          f <- 1/3 f + 2/3 s1 + 2/3 dt R(s1)
+        fa.mode = vl::FIELD_REQUIRE_ACTIVE | vl::FIELD_RECORD;
+        fa.phi = phi;
+        if ((rc = field(c, fa, s))) return rc;
+        st.in = sb;
+        st.fn = f;
+        st.out = f;
+        st.c0 = kRK3[1][0];
+        st.c1 = kRK3[1][1];
+        st.c2 = kRK3[1][2];
+        if ((rc = stage(c, st, s))) return rc;
+    }
+    return VL_OK;
+}
+
+}  // extern "C"
