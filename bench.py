@@ -37,7 +37,43 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kernel-reps", type=int, default=10)
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="launch each stage kind --kernel-reps times on --res (profiling target)")
+    ap.add_argument("--res", type=int, nargs=3, default=list(RES))
+    ap.add_argument("--order", type=int, default=ORDER)
+    ap.add_argument("--precision", choices=("fp64", "fp32"), default="fp64")
     return ap.parse_args()
+
+
+def kernel_only(args):
+    """Plain launches of the three fused stage kinds and one field solve (no graphs, no timing
+    of its own): the target of ncu captures of single kernels."""
+    import torch
+
+    from vlasov1d2v_b200 import problem
+    from vlasov1d2v_b200.context import get_context
+
+    torch.cuda.set_device(0)
+    res, n = tuple(args.res), args.order
+    p = problem.build(res, n, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=0,
+                      precision=args.precision)
+    ctx = get_context(p.grids, precision=args.precision, accel=p.refs.electron_acceleration_multiplier,
+                      bfield=p.elliptic.magnetic_field, kappa=p.elliptic.poisson_coefficient,
+                      courant=p.stepper.courant)
+    f = p.f.arr.as_subclass(torch.Tensor)
+    sa, sb = torch.empty_like(f), torch.empty_like(f)
+    ctx.sync_ghosts(f, sa)
+    ctx.sync_ghosts(f, sb)
+    E = p.elliptic.electric_field.as_subclass(torch.Tensor).contiguous()
+    dt = torch.tensor([1.0e-3], dtype=torch.float64, device=f.device)
+    for _ in range(args.kernel_reps):
+        ctx.rk_stage(0, f, None, sa, E, dt, partials=ctx.workspace)
+        ctx.rk_stage(1, sa, f, sb, E, dt, partials=ctx.workspace)
+        ctx.rk_stage(2, sb, f, sa, E, dt, partials=ctx.workspace)
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_only": True, "res": list(res), "order": n, "precision": args.precision,
+                      "reps": args.kernel_reps, "state_mb": f.numel() * f.element_size() / 1e6}))
+    return 0
 
 
 def dof(res, n):
@@ -276,6 +312,8 @@ class _TorchDist:
 
 def main():
     args = parse()
+    if args.kernel_only:
+        return kernel_only(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

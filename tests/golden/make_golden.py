@@ -152,7 +152,7 @@ def gen_small(name, res, order, nsteps, seed):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
-def gen_cfg1(nsteps=200):
+def gen_cfg1(nsteps=200, out_name="cfg1_200", summary=True):
     """Config 1 of the benchmark set: Nx = Nu = Nv = 16, n = 8, loss cone j = 6 times
     (1 + 0.01 cos kx), nsteps SSP-RK3 steps.  Stores the energy/dt/time histories and a
     compact summary of the final state."""
@@ -170,6 +170,10 @@ def gen_cfg1(nsteps=200):
     t0 = time.time()
     _steps(s, nsteps, out, keep_f=False)
     out["seconds"] = np.array(time.time() - t0)
+    out["blas_threads"] = np.array(int(os.environ.get("OPENBLAS_NUM_THREADS", "0")))
+    if not summary:
+        np.savez_compressed(os.path.join(HERE, f"{out_name}.npz"), **out)
+        return
     f = _np(s["f"].arr)
     out["final_rho"] = _np(s["f"].moment_zero())
     out["final_E"] = _np(s["el"].electric_field)
@@ -197,6 +201,10 @@ def main(argv):
         gen_small("n9", (2, 2, 2), 9, 1, seed=4)
     if "cfg1" in which:
         gen_cfg1()
+    if "cfg1_noise" in which:
+        # the same run with a different BLAS thread count: the reference's own summation-order
+        # noise floor for the energy history (run with OPENBLAS_NUM_THREADS=1)
+        gen_cfg1(out_name="cfg1_200_blas1", summary=False)
 
 
 if __name__ == "__main__":

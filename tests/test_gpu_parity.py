@@ -109,7 +109,8 @@ def test_main_loop_and_single_step_api(cuda, name):
 
     st.adapt_time_step(get_max_speeds(q.grids, q.elliptic, q.refs), q.grids.x.dx, q.grids.u.dx,
                        q.grids.v.dx)
-    assert st.dt == G2["dt"][0]
+    # dt comes from max|a E| of the initial field, itself within rounding of the reference's
+    assert abs(st.dt / G2["dt"][0] - 1) < 1e-14
     st.nonlinear_ssp_rk(q.f, q.basis, q.elliptic, q.grids, q.flux, q.refs)
     assert abs(st.dt / G2["dt"][1] - 1) < 1e-14
     assert rel_err(_np(q.f.arr)[INNER], G2["f_step1"]) < F_RTOL

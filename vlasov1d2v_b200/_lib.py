@@ -10,7 +10,7 @@ import os
 import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libvlasov1d2v.so")
+LIB_PATH = os.environ.get("VLASOV1D2V_LIB") or os.path.join(HERE, "libvlasov1d2v.so")
 
 VL_OK = 0
 VL_FP64 = 0

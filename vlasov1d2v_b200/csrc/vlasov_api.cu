@@ -3,9 +3,14 @@
 // Ownership: the context holds the immutable coefficient tables (device copies of the node
 // coordinates and DFT tensors, host copies of the small matrices that travel as kernel
 // parameters).  State, field, workspace and loop-state buffers belong to the caller.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <utility>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -13,6 +18,8 @@
 
 #include "vlasov1d2v.h"
 #include "vlasov_kernels.cuh"
+#include "vlasov_stage.cuh"
+#include "vlasov_stage_tma.cuh"
 
 struct vl_ctx {
     vl_config cfg;      // scalars (pointer members cleared)
@@ -29,6 +36,10 @@ struct vl_ctx {
     double *d_xw = nullptr;
     double2 *d_fwd = nullptr;
     double2 *d_inv = nullptr;
+    double *d_tables = nullptr;   // up [n n], xi [n 2], qw [n n]
+    int *d_err = nullptr;         // device error word of operators run without a loop state
+    bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
+    std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
 };
 
 namespace {
@@ -66,28 +77,86 @@ inline size_t elem_size(const vl_ctx *c) {
 // ------------------------------------------------------------------------------------------
 // stage kernel dispatch
 // ------------------------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 5-D view of the ghost-inclusive state: (v node, j, a, i, e), innermost first
 template <int N, typename T>
-int launch_stage_t(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
-    using G = vl::StageGeom<N>;
+int state_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
+    using G = vl::TmaGeom<N, T>;
+    auto key = std::make_pair(ptr, which);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2, X = c->cfg.nx + 2;
+    const cuuint64_t es = sizeof(T);
+    cuuint64_t dims[5] = {V * N, (cuuint64_t)N, U, (cuuint64_t)N, X};
+    cuuint64_t strides[4] = {V * N * es, V * N * N * es, V * N * N * U * es, V * N * N * U * N * es};
+    cuuint32_t box[5];
+    switch (which) {
+        case 0: box[0] = G::W; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
+        case 1: box[0] = G::COLS; box[1] = N; box[2] = 1; box[3] = 1; box[4] = 1; break;
+        case 2: box[0] = G::COLS; box[1] = 1; box[2] = 1; box[3] = N; box[4] = 1; break;
+        default: box[0] = G::COLS; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
+    }
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5,
+                     const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
+template <int N, typename T>
+int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageTables<T> tb;
     std::memset(&tb, 0, sizeof(tb));
     for (int i = 0; i < N * N; ++i) tb.up[i] = (T)c->up[i];
     for (int i = 0; i < 2 * N; ++i) tb.xi[i] = (T)c->xi[i];
     for (int i = 0; i < N * N; ++i) tb.qw[i] = c->qw[i];
-    const size_t smem = G::template smem_bytes<T>();
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaFuncSetAttribute(vl::stage_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        attr_done = true;
-    }
+    vl::StageArgs a = a0;
+    if (a.err == nullptr) a.err = c->d_err;
     dim3 grid(c->stage_grid_g, c->cfg.nx);
-    vl::stage_kernel<N, T><<<grid, vl::STAGE_THREADS, smem, s>>>(a, tb);
-    return check_launch("stage_kernel");
+    if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
+        if (c->use_tma) {
+            using G = vl::TmaGeom<N, T>;
+            vl::TmaMaps maps;
+            int rc;
+            if ((rc = state_map<N, T>(c, a.in, 0, &maps.in_tile))) return rc;
+            if ((rc = state_map<N, T>(c, a.in, 1, &maps.in_xface))) return rc;
+            if ((rc = state_map<N, T>(c, a.in, 2, &maps.in_uface))) return rc;
+            if ((rc = state_map<N, T>(c, a.fn ? a.fn : a.in, 3, &maps.fn_tile))) return rc;
+            vl::stage_tma_kernel<N, T><<<grid, G::THREADS, G::smem_bytes(), s>>>(a, tb, maps);
+            return check_launch("stage_tma_kernel");
+        }
+    }
+    using G = vl::PencilGeom<N, T>;
+    vl::stage_pencil_kernel<N, T><<<grid, G::THREADS, G::smem_bytes(), s>>>(a, tb);
+    return check_launch("stage_pencil_kernel");
 }
 
 template <typename T>
-int launch_stage(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
+int launch_stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
     switch (c->cfg.n) {
         case 1: return launch_stage_t<1, T>(c, a, s);
         case 2: return launch_stage_t<2, T>(c, a, s);
@@ -103,55 +172,73 @@ int launch_stage(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
     }
 }
 
-int stage(const vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
+int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
     return c->cfg.precision == VL_FP64 ? launch_stage<double>(c, a, s)
                                        : launch_stage<float>(c, a, s);
 }
 
 template <int N, typename T>
-int stage_occupancy_t() {
-    using G = vl::StageGeom<N>;
+int stage_occupancy_t(bool tma) {
     int blocks = 0;
-    const size_t smem = G::template smem_bytes<T>();
-    cudaFuncSetAttribute(vl::stage_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_kernel<N, T>,
-                                                      vl::STAGE_THREADS, smem) != cudaSuccess)
+    if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
+        if (tma) {
+            using G = vl::TmaGeom<N, T>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_tma_kernel<N, T>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_tma_kernel<N, T>,
+                                                              G::THREADS, smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
+    }
+    using G = vl::PencilGeom<N, T>;
+    const size_t smem = G::smem_bytes();
+    cudaFuncSetAttribute(vl::stage_pencil_kernel<N, T>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_pencil_kernel<N, T>,
+                                                      G::THREADS, smem) != cudaSuccess)
         return 1;
     return blocks > 0 ? blocks : 1;
 }
 
+template <int N, typename T>
+bool tma_supported_t(const vl_config &g) {
+    if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
+        return ((size_t)(g.nv + 2) * N * sizeof(T)) % 16 == 0;
+    }
+    return false;
+}
+
 template <typename T>
-int stage_occupancy(int n) {
+int stage_occupancy(int n, bool tma) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>();
-        case 2: return stage_occupancy_t<2, T>();
-        case 3: return stage_occupancy_t<3, T>();
-        case 4: return stage_occupancy_t<4, T>();
-        case 5: return stage_occupancy_t<5, T>();
-        case 6: return stage_occupancy_t<6, T>();
-        case 7: return stage_occupancy_t<7, T>();
-        case 8: return stage_occupancy_t<8, T>();
-        case 9: return stage_occupancy_t<9, T>();
-        case 10: return stage_occupancy_t<10, T>();
+        case 1: return stage_occupancy_t<1, T>(tma);
+        case 2: return stage_occupancy_t<2, T>(tma);
+        case 3: return stage_occupancy_t<3, T>(tma);
+        case 4: return stage_occupancy_t<4, T>(tma);
+        case 5: return stage_occupancy_t<5, T>(tma);
+        case 6: return stage_occupancy_t<6, T>(tma);
+        case 7: return stage_occupancy_t<7, T>(tma);
+        case 8: return stage_occupancy_t<8, T>(tma);
+        case 9: return stage_occupancy_t<9, T>(tma);
+        case 10: return stage_occupancy_t<10, T>(tma);
         default: return 1;
     }
 }
 
-int stage_bt(int n) {
-    switch (n) {
-        case 1: return vl::StageGeom<1>::BT;
-        case 2: return vl::StageGeom<2>::BT;
-        case 3: return vl::StageGeom<3>::BT;
-        case 4: return vl::StageGeom<4>::BT;
-        case 5: return vl::StageGeom<5>::BT;
-        case 6: return vl::StageGeom<6>::BT;
-        case 7: return vl::StageGeom<7>::BT;
-        case 8: return vl::StageGeom<8>::BT;
-        case 9: return vl::StageGeom<9>::BT;
-        default: return vl::StageGeom<10>::BT;
+template <typename T>
+bool tma_supported(const vl_config &g) {
+    switch (g.n) {
+        case 2: return tma_supported_t<2, T>(g);
+        case 4: return tma_supported_t<4, T>(g);
+        case 8: return tma_supported_t<8, T>(g);
+        default: return false;
     }
 }
+
+// v elements per tile of the stage kernel
+int stage_epw(int n) { return 32 / n; }
 
 // ------------------------------------------------------------------------------------------
 // moment kernel dispatch
@@ -247,6 +334,7 @@ vl::StageArgs stage_args(const vl_ctx *c) {
     std::memset(&a, 0, sizeof(a));
     a.u_nodes = c->d_unodes;
     a.v_nodes = c->d_vnodes;
+    a.tables = c->d_tables;
     a.nx = c->cfg.nx;
     a.nu = c->cfg.nu;
     a.nv = c->cfg.nv;
@@ -294,6 +382,9 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     const size_t elems = (size_t)(cfg->nx + 2) * cfg->n * (cfg->nu + 2) * cfg->n *
                          (cfg->nv + 2) * cfg->n;
     if (elems >= ((size_t)1 << 40)) return fail(VL_ERR_TOO_LARGE, "state too large");
+    // offsets inside one x slab are 32-bit in the stage kernel
+    if (elems / (size_t)(cfg->nx + 2) >= ((size_t)1 << 31))
+        return fail(VL_ERR_TOO_LARGE, "one x slab of the state exceeds 2^31 elements");
 
     vl_ctx *c = new vl_ctx();
     c->cfg = *cfg;
@@ -327,10 +418,32 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     const size_t tbytes = sizeof(double2) * (size_t)cfg->nx * n * cfg->n_modes;
     if ((rc = upload(&c->d_fwd, cfg->dft_fwd, tbytes))) return cleanup(rc);
     if ((rc = upload(&c->d_inv, cfg->dft_inv, tbytes))) return cleanup(rc);
+    {
+        std::vector<double> tabs((size_t)2 * n * n + 2 * n);
+        std::memcpy(tabs.data(), c->up, sizeof(double) * n * n);
+        std::memcpy(tabs.data() + n * n, c->xi, sizeof(double) * 2 * n);
+        std::memcpy(tabs.data() + n * n + 2 * n, c->qw, sizeof(double) * n * n);
+        if ((rc = upload(&c->d_tables, tabs.data(), sizeof(double) * tabs.size()))) return cleanup(rc);
+    }
 
+    {
+        int *e0 = nullptr;
+        cudaError_t ee = cudaMalloc((void **)&e0, sizeof(int));
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMalloc(err)"));
+        c->d_err = e0;
+        ee = cudaMemset(c->d_err, 0, sizeof(int));
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMemset(err)"));
+    }
+    c->use_tma = (cfg->precision == VL_FP64 ? tma_supported<double>(*cfg) : tma_supported<float>(*cfg)) &&
+                 encode_fn() != nullptr;
+    {
+        const char *env = getenv("VLASOV1D2V_NO_TMA");
+        if (env && env[0] == '1') c->use_tma = false;
+    }
     // CTAs per x element: fill the device (resident CTAs x SMs), at most one per tile
-    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n) : stage_occupancy<float>(n);
-    const int bt = stage_bt(n);
+    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma)
+                                              : stage_occupancy<float>(n, c->use_tma);
+    const int bt = stage_epw(n);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     int g = (c->sm_count * occ + cfg->nx - 1) / cfg->nx;
     if (g > tiles) g = tiles;
@@ -348,6 +461,8 @@ int vl_ctx_destroy(vl_ctx *c) {
     cudaFree(c->d_xw);
     cudaFree(c->d_fwd);
     cudaFree(c->d_inv);
+    cudaFree(c->d_tables);
+    cudaFree(c->d_err);
     delete c;
     return VL_OK;
 }

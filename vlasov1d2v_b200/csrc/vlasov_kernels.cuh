@@ -6,9 +6,7 @@
 // A DG element is an n^3 block; its six face traces are the adjacent node planes.
 //
 // Kernels
-//   stage_kernel    one fused SSP-RK stage (or a bare RHS): the three n x n "up" contractions,
-//                   the upwind face lifts in x, u and v, the Jacobian-weighted sum, the RK
-//                   linear combination and the zeroth-moment partials of the result.
+//   stage kernel    (vlasov_stage.cuh) one fused SSP-RK stage or a bare RHS.
 //   moment_kernel   standalone zeroth velocity moment, one CTA per (x element, x node).
 //   field_kernel    one CTA: moment partials -> density -> mean-subtracted charge -> forward
 //                   high-order DFT -> spectral E and phi -> inverse DFT at the LGL nodes ->
@@ -23,7 +21,6 @@
 namespace vl {
 
 constexpr int NMAX = 10;
-constexpr int STAGE_THREADS = 256;
 
 enum StageKind : int { KIND_EULER = 0, KIND_COMBINE = 1, KIND_RHS = 2 };
 
@@ -48,6 +45,8 @@ struct StageArgs {
     const double *u_nodes; // [(nu+2) n]
     const double *v_nodes; // [(nv+2) n]
     double *partials;      // [nx][G][n] moment partials of out, or null
+    const double *tables;  // device copy: up [n n], xi [n 2], qw [n n] (per-lane indexed reads)
+    int *err;              // device error word: bit 1 = a bounded wait timed out
     int nx, nu, nv;
     int xhalo;
     int kind;
@@ -81,241 +80,6 @@ __device__ __forceinline__ dd shfl_down_dd(dd v, int off) {
     r.hi = __shfl_down_sync(0xffffffffu, v.hi, off);
     r.lo = __shfl_down_sync(0xffffffffu, v.lo, off);
     return r;
-}
-
-// ----------------------------------------------------------------------------------------------
-// fused stage kernel
-// ----------------------------------------------------------------------------------------------
-template <int N>
-struct StageGeom {
-    static constexpr int BT = (256 / (N * N)) < 1 ? 1 : ((256 / (N * N)) > 64 ? 64 : (256 / (N * N)));
-    static constexpr int W = BT * N;          // tile width in v nodes
-    static constexpr int RS = (W + 2) | 1;    // input row stride (odd: conflict-free columns)
-    static constexpr int AS = W | 1;          // accumulator row stride
-    template <typename T>
-    static constexpr size_t smem_bytes() {
-        return sizeof(T) * (size_t)(N * N * RS + N * N * AS + 2 * N * W);
-    }
-};
-
-template <int N, typename T>
-__global__ void __launch_bounds__(STAGE_THREADS)
-stage_kernel(const StageArgs a, const StageTables<T> tb) {
-    using G = StageGeom<N>;
-    constexpr int BT = G::BT, W = G::W, RS = G::RS, AS = G::AS;
-    if (a.state != nullptr && a.state->active == 0) return;
-
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *sIn = reinterpret_cast<T *>(smem_raw);
-    T *sAcc = sIn + N * N * RS;
-    T *sXh = sAcc + N * N * AS;
-    T *sUh = sXh + N * W;
-
-    const T *__restrict__ in = static_cast<const T *>(a.in);
-    const T *fn = static_cast<const T *>(a.fn);
-    T *out = static_cast<T *>(a.out);
-    T *gout = static_cast<T *>(a.ghost_out);
-
-    const int nx = a.nx, nu = a.nu, nv = a.nv;
-    const int U = nu + 2, V = nv + 2;
-    const size_t sJ = (size_t)V * N;     // stride of node index j
-    const size_t sA = sJ * N;            // stride of u element
-    const size_t sI = sA * U;            // stride of node index i
-    const size_t sE = sI * N;            // stride of x element
-
-    const int e = blockIdx.y;
-    const int g = blockIdx.x, Gn = gridDim.x;
-    const int tid = threadIdx.x;
-    const int nbt = (nv + BT - 1) / BT;
-    const int tiles = nu * nbt;
-
-    const int Eg = e + 1;
-    int El, Er;
-    if (a.xhalo == VL_XHALO_PERIODIC) {
-        El = (e == 0) ? nx : e;
-        Er = (e == nx - 1) ? 1 : e + 2;
-    } else {
-        El = e;
-        Er = e + 2;
-    }
-
-    const double dtd = (a.kind == KIND_RHS) ? 0.0 : *a.dt;
-    const T dtT = (T)dtd;
-    const T c0 = (T)a.c0, c1 = (T)a.c1;
-    const T c2dt = (T)(a.c2 * dtd);
-    const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
-    const double accel = a.accel, bfield = a.bfield;
-    const double nbfield = -bfield;
-
-    double mom[N];
-#pragma unroll
-    for (int i = 0; i < N; ++i) mom[i] = 0.0;
-
-    for (int t = g; t < tiles; t += Gn) {
-        const int au = t / nbt;
-        const int b0 = (t % nbt) * BT;
-        const int nb = min(BT, nv - b0);
-        const int w = nb * N;
-        const int Ag = au + 1;
-        const size_t col0 = (size_t)(b0 + 1) * N;   // first interior column of the tile
-        const size_t rowE = (size_t)Eg * sE + (size_t)Ag * sA;
-
-        // ---- load the tile and its v halo columns (contiguous rows) ----
-        for (int idx = tid; idx < N * N * (w + 2); idx += STAGE_THREADS) {
-            const int r = idx / (w + 2);
-            const int c = idx - r * (w + 2);
-            const int i = r / N, j = r - (r / N) * N;
-            sIn[r * RS + c] = in[rowE + (size_t)i * sI + (size_t)j * sJ + col0 - 1 + c];
-        }
-        // ---- x halo: one upwind trace per x line (j, c) ----
-        for (int idx = tid; idx < N * w; idx += STAGE_THREADS) {
-            const int j = idx / w;
-            const int c = idx - j * w;
-            const double uj = a.u_nodes[Ag * N + j];
-            const size_t src = (uj >= 0.0)
-                ? (size_t)El * sE + (size_t)(N - 1) * sI + (size_t)Ag * sA + (size_t)j * sJ
-                : (size_t)Er * sE + (size_t)Ag * sA + (size_t)j * sJ;
-            sXh[j * W + c] = in[src + col0 + c];
-        }
-        // ---- u halo: one upwind trace per u line (i, c) ----
-        for (int idx = tid; idx < N * w; idx += STAGE_THREADS) {
-            const int i = idx / w;
-            const int c = idx - i * w;
-            const int bk = (b0 + 1) * N + c;
-            const double s = accel * (a.E[Eg * N + i] + bfield * a.v_nodes[bk]);
-            const size_t src = (s >= 0.0)
-                ? (size_t)Eg * sE + (size_t)i * sI + (size_t)(Ag - 1) * sA + (size_t)(N - 1) * sJ
-                : (size_t)Eg * sE + (size_t)i * sI + (size_t)(Ag + 1) * sA;
-            sUh[i * W + c] = in[src + col0 + c];
-        }
-        __syncthreads();
-
-        // ---- v pass: lines along k for each (element bl, i, j) ----
-        for (int l = tid; l < nb * N * N; l += STAGE_THREADS) {
-            const int j = l % N;
-            const int i = (l / N) % N;
-            const int bl = l / (N * N);
-            const T *p = sIn + (i * N + j) * RS + 1 + bl * N;
-            T f[N];
-#pragma unroll
-            for (int k = 0; k < N; ++k) f[k] = p[k];
-            const T left_nb = p[-1];
-            const T right_nb = p[N];
-            const double sv_d = accel * (nbfield * a.u_nodes[Ag * N + j]);
-            const T sv = (T)sv_d;
-            const bool pos = sv_d >= 0.0;
-            const T hL = pos ? left_nb : f[0];
-            const T hR = pos ? f[N - 1] : right_nb;
-            T *q = sAcc + (i * N + j) * AS + bl * N;
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                T d = (T)0;
-#pragma unroll
-                for (int m = 0; m < N; ++m) d = fma(tb.up[k * N + m], f[m], d);
-                d = fma(tb.xi[2 * k], hL, d);
-                d = fma(-tb.xi[2 * k + 1], hR, d);
-                q[k] = (sv * d) * jv;
-            }
-        }
-        __syncthreads();
-
-        // ---- u pass: lines along j for each (i, column c) ----
-        for (int l = tid; l < N * w; l += STAGE_THREADS) {
-            const int i = l / w;
-            const int c = l - i * w;
-            T f[N];
-#pragma unroll
-            for (int m = 0; m < N; ++m) f[m] = sIn[(i * N + m) * RS + c + 1];
-            const T nbv = sUh[i * W + c];
-            const int bk = (b0 + 1) * N + c;
-            const double s_d = accel * (a.E[Eg * N + i] + bfield * a.v_nodes[bk]);
-            const T s = (T)s_d;
-            const bool pos = s_d >= 0.0;
-            const T hL = pos ? nbv : f[0];
-            const T hR = pos ? f[N - 1] : nbv;
-#pragma unroll
-            for (int jj = 0; jj < N; ++jj) {
-                T d = (T)0;
-#pragma unroll
-                for (int m = 0; m < N; ++m) d = fma(tb.up[jj * N + m], f[m], d);
-                d = fma(tb.xi[2 * jj], hL, d);
-                d = fma(-tb.xi[2 * jj + 1], hR, d);
-                T *q = sAcc + (i * N + jj) * AS + c;
-                *q = fma(s * d, ju, *q);
-            }
-        }
-        __syncthreads();
-
-        // ---- x pass + RK combination + moment partials: lines along i for each (j, c) ----
-        for (int l = tid; l < N * w; l += STAGE_THREADS) {
-            const int j = l / w;
-            const int c = l - j * w;
-            const int k = c % N;
-            T f[N];
-#pragma unroll
-            for (int m = 0; m < N; ++m) f[m] = sIn[(m * N + j) * RS + c + 1];
-            const T nbv = sXh[j * W + c];
-            const double u_d = a.u_nodes[Ag * N + j];
-            const T u = (T)u_d;
-            const bool pos = u_d >= 0.0;
-            const T hL = pos ? nbv : f[0];
-            const T hR = pos ? f[N - 1] : nbv;
-            const size_t base = (size_t)Eg * sE + (size_t)Ag * sA + (size_t)j * sJ + col0 + c;
-            const double wq = tb.qw[j * N + k];
-#pragma unroll
-            for (int ii = 0; ii < N; ++ii) {
-                T d = (T)0;
-#pragma unroll
-                for (int m = 0; m < N; ++m) d = fma(tb.up[ii * N + m], f[m], d);
-                d = fma(tb.xi[2 * ii], hL, d);
-                d = fma(-tb.xi[2 * ii + 1], hR, d);
-                const T r = fma(u * d, jx, sAcc[(ii * N + j) * AS + c]);
-                T o;
-                const size_t off = base + (size_t)ii * sI;
-                if (a.kind == KIND_RHS) {
-                    o = r;
-                } else if (a.kind == KIND_EULER) {
-                    o = fma(dtT, r, f[ii]);
-                } else {
-                    o = fma(c2dt, r, fma(c1, f[ii], c0 * fn[off]));
-                }
-                out[off] = o;
-                mom[ii] = fma(wq, (double)o, mom[ii]);
-            }
-            if (gout != nullptr) {
-                // periodic x-ghost refresh of f: slab 0 <- slab nx, slab nx+1 <- slab 1
-                // (Distribution.swap_ghost_cells_of_array, main/grid.py:187-189)
-                if (e == nx - 1) {
-#pragma unroll
-                    for (int ii = 0; ii < N; ++ii) gout[base - (size_t)Eg * sE + (size_t)ii * sI] = f[ii];
-                }
-                if (e == 0) {
-#pragma unroll
-                    for (int ii = 0; ii < N; ++ii)
-                        gout[base - (size_t)Eg * sE + (size_t)(nx + 1) * sE + (size_t)ii * sI] = f[ii];
-                }
-            }
-        }
-        __syncthreads();
-    }
-
-    if (a.partials == nullptr) return;
-    // ---- CTA reduction of the moment partials (double-double) ----
-    __shared__ dd red[STAGE_THREADS / 32][N];
-    const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        dd v = {mom[i], 0.0};
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_down_dd(v, off));
-        if (lane == 0) red[warp][i] = v;
-    }
-    __syncthreads();
-    if (tid < N) {
-        dd s = red[0][tid];
-        for (int w8 = 1; w8 < STAGE_THREADS / 32; ++w8) s = dd_add(s, red[w8][tid]);
-        a.partials[((size_t)e * Gn + g) * N + tid] = s.hi + s.lo;
-    }
 }
 
 // ----------------------------------------------------------------------------------------------
