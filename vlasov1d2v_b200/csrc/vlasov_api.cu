@@ -109,11 +109,14 @@ int state_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     cuuint64_t strides[4] = {V * N * es, V * N * N * es, V * N * N * U * es, V * N * N * U * N * es};
     cuuint32_t box[5];
     switch (which) {
-        case 0: box[0] = G::W; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
+        case 0: case 5: box[0] = G::W; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
         case 1: box[0] = G::COLS; box[1] = N; box[2] = 1; box[3] = 1; box[4] = 1; break;
         case 2: box[0] = G::COLS; box[1] = 1; box[2] = 1; box[3] = N; box[4] = 1; break;
         default: box[0] = G::COLS; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
     }
+    // output tiles: the v extent ends after the last interior element, so stores of a ragged
+    // last tile are clipped before the v ghost element
+    if (which == 4) dims[0] = (cuuint64_t)(c->cfg.nv + 1) * N;
     cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     CUtensorMap m;
     CUresult r = enc(&m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5,
@@ -134,6 +137,14 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     for (int i = 0; i < N * N; ++i) tb.up[i] = (T)c->up[i];
     for (int i = 0; i < 2 * N; ++i) tb.xi[i] = (T)c->xi[i];
     for (int i = 0; i < N * N; ++i) tb.qw[i] = c->qw[i];
+    for (int i = 0; i < N; ++i)
+        for (int m = 0; m < N; ++m) {
+            double p = c->up[i * N + m], q = c->up[i * N + m];
+            if (m == N - 1) p -= c->xi[2 * i + 1];
+            if (m == 0) q += c->xi[2 * i];
+            tb.upP[i * N + m] = (T)p;
+            tb.upM[i * N + m] = (T)q;
+        }
     vl::StageArgs a = a0;
     if (a.err == nullptr) a.err = c->d_err;
     dim3 grid(c->stage_grid_g, c->cfg.nx);
@@ -445,7 +456,9 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
                                               : stage_occupancy<float>(n, c->use_tma);
     const int bt = stage_epw(n);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
-    int g = (c->sm_count * occ + cfg->nx - 1) / cfg->nx;
+    // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double
+    // the kernel time)
+    int g = (c->sm_count * occ) / cfg->nx;
     if (g > tiles) g = tiles;
     if (g < 1) g = 1;
     c->stage_grid_g = g;

@@ -32,6 +32,11 @@ struct StageTables {
     T up[NMAX * NMAX];     // up[i][j]        (main/basis.py:176-188)
     T xi[NMAX * 2];        // xi[i][face]     (main/basis.py:110)
     double qw[NMAX * NMAX];  // w_j w_k / (J_u J_v)  (main/grid.py:297-301)
+    // up with the own-trace lift folded in, per upwind direction:
+    //   speed >= 0: d = sum_m upP[i][m] f[m] + xi[i][0] * (left neighbour trace)
+    //   speed <  0: d = sum_m upM[i][m] f[m] - xi[i][1] * (right neighbour trace)
+    T upP[NMAX * NMAX];
+    T upM[NMAX * NMAX];
 };
 
 struct StageArgs {

@@ -211,7 +211,6 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
 #pragma unroll
             for (int jc = 0; jc < JC; ++jc) fn_cur[jc] = (jc < JN) ? pfn[(J0 + jc) * sJ] : (T)0;
         }
-        double mom_row = 0.0;
 #pragma unroll 1
         for (int i = 0; i < N; ++i) {
             const int inext = (i + 1 < N) ? i + 1 : i;
@@ -277,7 +276,7 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
                 dv = fma(xik0, vL, dv);
                 dv = fma(-xik1, vR, dv);
                 const T r = fma((T)ux[jc] * dx, jx, fma(s * du, ju, ((T)sv_d * dv) * jv));
-                const T fij = row[j];
+                const T fij = rp[j * RW];
                 T o;
                 if (kind == KIND_RHS) {
                     o = r;
@@ -296,7 +295,6 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
                 for (int jc = 0; jc < JC; ++jc) fn_cur[jc] = fn_next[jc];
             }
         }
-        (void)mom_row;
         if (gout != nullptr && (e == nx - 1 || e == 0)) {
             // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
 #pragma unroll

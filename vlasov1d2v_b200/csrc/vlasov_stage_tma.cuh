@@ -21,6 +21,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "vlasov_kernels.cuh"
 
 #ifndef VL_TMA_JC64
@@ -28,6 +30,11 @@
 #endif
 #ifndef VL_TMA_JC32
 #define VL_TMA_JC32 4
+#endif
+// 1: f^n tiles stream through shared memory with TMA; 0: each thread reads its f^n values
+// straight from global memory (less shared memory per CTA, more resident CTAs)
+#ifndef VL_TMA_STAGE_FN
+#define VL_TMA_STAGE_FN 1
 #endif
 
 namespace vl {
@@ -39,14 +46,17 @@ struct TmaGeom {
     static constexpr int COLS = EPW * N;
     static constexpr int W = COLS + 2 * P;                    // IN row length
     static constexpr int JC = sizeof(T) == 8 ? VL_TMA_JC64 : VL_TMA_JC32;
+    static constexpr bool SUPPORTED_SHAPE = ((N * (int)sizeof(T)) % 16 == 0) && (32 % N == 0);
     static constexpr int NW = (N + JC - 1) / JC;               // warps
+    static_assert(!SUPPORTED_SHAPE || NW <= 8, "at most 8 j chunks per tile");
     static constexpr int THREADS = 32 * NW;
     static constexpr int VEC = (sizeof(T) == 8) ? ((N % 2 == 0) ? 2 : 1) : ((N % 4 == 0) ? 4 : 1);
-    static constexpr bool SUPPORTED = ((N * (int)sizeof(T)) % 16 == 0) && (32 % N == 0);
+    static constexpr bool SUPPORTED = SUPPORTED_SHAPE;
     // stage layout (bytes, 128-aligned pieces)
     static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
     static constexpr size_t IN_B = al(sizeof(T) * (size_t)W * N * N);
-    static constexpr size_t FN_B = al(sizeof(T) * (size_t)COLS * N * N);
+    static constexpr bool STAGE_FN = VL_TMA_STAGE_FN != 0;
+    static constexpr size_t FN_B = STAGE_FN ? al(sizeof(T) * (size_t)COLS * N * N) : 0;
     static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * COLS * N);
     static constexpr size_t UF_B = al(sizeof(T) * (size_t)2 * COLS * N);
     static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B;
@@ -106,8 +116,35 @@ __device__ __forceinline__ void tma_load_5d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+#ifndef VL_SPLIT_SUM
+#define VL_SPLIT_SUM 0
+#endif
+#ifndef VL_TMA_MINB
+#define VL_TMA_MINB 1
+#endif
+
+// sum_m coef(m) v[m] with two interleaved partial sums (halves the FMA dependency chain)
+template <int N, typename T, typename C>
+__device__ __forceinline__ T dot_n(C coef, const T (&v)[N]) {
+    if constexpr (VL_SPLIT_SUM && N >= 4) {
+        T s0 = (T)0, s1 = (T)0;
+#pragma unroll
+        for (int m = 0; m + 1 < N; m += 2) {
+            s0 = fma(coef(m), v[m], s0);
+            s1 = fma(coef(m + 1), v[m + 1], s1);
+        }
+        if constexpr (N % 2) s0 = fma(coef(N - 1), v[N - 1], s0);
+        return s0 + s1;
+    } else {
+        T s = (T)0;
+#pragma unroll
+        for (int m = 0; m < N; ++m) s = fma(coef(m), v[m], s);
+        return s;
+    }
+}
+
 template <int N, typename T>
-__global__ void __launch_bounds__(TmaGeom<N, T>::THREADS)
+__global__ void __launch_bounds__(TmaGeom<N, T>::THREADS, VL_TMA_MINB)
 stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                  const __grid_constant__ TmaMaps maps) {
     using G = TmaGeom<N, T>;
@@ -124,8 +161,7 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int J0 = (tid >> 5) * JC;
-    const int JN = min(JC, N - J0);
+    const int warp = tid >> 5;
     const int c = lane;                     // column
     const int bl = c / N, k = c - (c / N) * N;
     const bool lane_ok = c < COLS;
@@ -145,7 +181,7 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     }
     const int kind = a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
-    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0);
+    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + ((with_fn && G::STAGE_FN) ? G::TX_FN : 0);
     const int nbt = (nv + EPW - 1) / EPW;
     const int tiles = nu * nbt;
     const int ntile_cta = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -177,7 +213,7 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     Eg);
         tma_load_5d(st + G::IN_B + G::FN_B + G::XF_B + sizeof(T) * COLS * N, &maps.in_uface, &full[s],
                     x0, 0, Ag + 1, 0, Eg);
-        if (with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0, 0, Ag, 0, Eg);
+        if (G::STAGE_FN && with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0, 0, Ag, 0, Eg);
     };
     if (tid == 0) {
         if (ntile_cta > 0) issue(0, 0);
@@ -193,9 +229,6 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
 #pragma unroll
     for (int m = 0; m < N; ++m) upk[m] = tb.up[kk * N + m];
     const T xik0 = tb.xi[2 * kk], xik1 = tb.xi[2 * kk + 1];
-    double wk[JC];
-#pragma unroll
-    for (int jc = 0; jc < JC; ++jc) wk[jc] = (jc < JN && lane_ok) ? tb.qw[(J0 + jc) * N + kk] : 0.0;
     T *out = static_cast<T *>(a.out);
     T *gout = static_cast<T *>(a.ghost_out);
 
@@ -217,22 +250,39 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
         const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
 
-        if (act) {
+        auto tile_body = [&](auto wj) {
+            constexpr int J0 = decltype(wj)::value * JC;
+            constexpr int JN = (J0 + JC <= N) ? JC : (N - J0);
+            double wk[JC];
+#pragma unroll
+            for (int jc = 0; jc < JC; ++jc) wk[jc] = (jc < JN && lane_ok) ? tb.qw[(J0 + jc) * N + kk] : 0.0;
             double ux[JC];
             T f[N][JC];
             T xh[JC];
 #pragma unroll
-            for (int jc = 0; jc < JC; ++jc) {
-                const int j = J0 + (jc < JN ? jc : 0);
+            for (int jc = 0; jc < JN; ++jc) {
+                const int j = J0 + jc;
                 ux[jc] = a.u_nodes[Ag * N + j];
 #pragma unroll
                 for (int m = 0; m < N; ++m) f[m][jc] = sIn[(m * N + j) * W + P + c];
                 xh[jc] = sXF[((ux[jc] >= 0.0) ? 0 : COLS * N) + j * COLS + c];
             }
+            if (gout != nullptr && (e == nx - 1 || e == 0)) {
+                // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
+                T *pg = gout + (size_t)Ag * sA + col;
+#pragma unroll
+                for (int jc = 0; jc < JN; ++jc) {
+                    const int j = J0 + jc;
+#pragma unroll
+                    for (int m = 0; m < N; ++m) {
+                        if (e == nx - 1) pg[m * sI + j * sJ] = f[m][jc];
+                        if (e == 0) pg[(size_t)(nx + 1) * sE_ + m * sI + j * sJ] = f[m][jc];
+                    }
+                }
+            }
             const double vnode = a.v_nodes[col];
             T *pout = out + (size_t)Eg * sE_ + (size_t)Ag * sA + col;
-            double mloc[1] = {0.0};
-            (void)mloc;
+            const T *pfn = static_cast<const T *>(a.fn) + ((size_t)Eg * sE_ + (size_t)Ag * sA + col);
 #pragma unroll 1
             for (int i = 0; i < N; ++i) {
                 T row[N];
@@ -246,34 +296,32 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                 const T uR = upos ? row[N - 1] : uh;
                 double mrow = 0.0;
 #pragma unroll
-                for (int jc = 0; jc < JC; ++jc) {
-                    if (jc >= JN) break;
+                for (int jc = 0; jc < JN; ++jc) {
                     const int j = J0 + jc;
-                    T du = (T)0;
-#pragma unroll
-                    for (int m = 0; m < N; ++m) du = fma(tb.up[j * N + m], row[m], du);
+                    T du = dot_n<N, T>([&](int m) { return tb.up[j * N + m]; }, row);
                     du = fma(tb.xi[2 * j], uL, du);
                     du = fma(-tb.xi[2 * j + 1], uR, du);
                     const bool xpos = ux[jc] >= 0.0;
                     const T xL = xpos ? xh[jc] : f[0][jc];
                     const T xR = xpos ? f[N - 1][jc] : xh[jc];
-                    T dx = (T)0;
+                    T colv[N];
 #pragma unroll
-                    for (int m = 0; m < N; ++m) dx = fma(tb.up[i * N + m], f[m][jc], dx);
+                    for (int m = 0; m < N; ++m) colv[m] = f[m][jc];
+                    T dx = dot_n<N, T>([&](int m) { return tb.up[i * N + m]; }, colv);
                     dx = fma(tb.xi[2 * i], xL, dx);
                     dx = fma(-tb.xi[2 * i + 1], xR, dx);
                     const T *lp = sIn + (i * N + j) * W + P + bl * N;
                     T line[N];
                     load_line<N, VEC, T>(lp, line);
                     const double sv_d = accel * (nbfield * ux[jc]);
-                    const bool vpos = sv_d >= 0.0;
-                    const T vL = vpos ? lp[-1] : line[0];
-                    const T vR = vpos ? line[N - 1] : lp[N];
-                    T dv = (T)0;
-#pragma unroll
-                    for (int m = 0; m < N; ++m) dv = fma(upk[m], line[m], dv);
-                    dv = fma(xik0, vL, dv);
-                    dv = fma(-xik1, vR, dv);
+                    T dv = dot_n<N, T>([&](int m) { return upk[m]; }, line);
+                    if (sv_d >= 0.0) {   // warp-uniform: upwind side of the v faces
+                        dv = fma(xik0, lp[-1], dv);
+                        dv = fma(-xik1, line[N - 1], dv);
+                    } else {
+                        dv = fma(xik0, line[0], dv);
+                        dv = fma(-xik1, lp[N], dv);
+                    }
                     const T r = fma((T)ux[jc] * dx, jx, fma(sp * du, ju, ((T)sv_d * dv) * jv));
                     const T fij = row[j];
                     T o;
@@ -282,26 +330,26 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     } else if (kind == KIND_EULER) {
                         o = fma(dtT, r, fij);
                     } else {
-                        o = fma(c2dt, r, fma(c1, fij, c0 * sFn[(i * N + j) * COLS + c]));
+                        const T fnv = G::STAGE_FN ? sFn[(i * N + j) * COLS + c] : pfn[i * sI + j * sJ];
+                        o = fma(c2dt, r, fma(c1, fij, c0 * fnv));
                     }
                     pout[i * sI + j * sJ] = o;
                     mrow = fma(wk[jc], (double)o, mrow);
                 }
                 sMom[i * NT + tid] += mrow;
             }
-            if (gout != nullptr && (e == nx - 1 || e == 0)) {
-                // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
-                T *pg = gout + (size_t)Ag * sA + col;
-#pragma unroll
-                for (int jc = 0; jc < JC; ++jc) {
-                    if (jc >= JN) break;
-                    const int j = J0 + jc;
-#pragma unroll
-                    for (int m = 0; m < N; ++m) {
-                        if (e == nx - 1) pg[m * sI + j * sJ] = f[m][jc];
-                        if (e == 0) pg[(size_t)(nx + 1) * sE_ + m * sI + j * sJ] = f[m][jc];
-                    }
-                }
+        };
+        if (act) {
+            switch (warp) {
+                case 0: tile_body(std::integral_constant<int, 0>{}); break;
+                case 1: if constexpr (G::NW > 1) tile_body(std::integral_constant<int, (G::NW > 1 ? 1 : 0)>{}); break;
+                case 2: if constexpr (G::NW > 2) tile_body(std::integral_constant<int, (G::NW > 2 ? 2 : 0)>{}); break;
+                case 3: if constexpr (G::NW > 3) tile_body(std::integral_constant<int, (G::NW > 3 ? 3 : 0)>{}); break;
+                case 4: if constexpr (G::NW > 4) tile_body(std::integral_constant<int, (G::NW > 4 ? 4 : 0)>{}); break;
+                case 5: if constexpr (G::NW > 5) tile_body(std::integral_constant<int, (G::NW > 5 ? 5 : 0)>{}); break;
+                case 6: if constexpr (G::NW > 6) tile_body(std::integral_constant<int, (G::NW > 6 ? 6 : 0)>{}); break;
+                case 7: if constexpr (G::NW > 7) tile_body(std::integral_constant<int, (G::NW > 7 ? 7 : 0)>{}); break;
+                default: break;
             }
         }
         __syncthreads();   // stage s fully consumed
