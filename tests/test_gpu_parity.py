@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 import torch
 
-from helpers import F_RTOL, INNER, SMALL_CASES, case_setup, field_rtol, golden, rel_err
+from helpers import F_RTOL, INNER, SMALL_CASES, case_setup, field_rtol, golden, history_err, rel_err
 from oracle import vlasov_oracle as vo
 
 pytestmark = pytest.mark.gpu
@@ -189,8 +189,12 @@ def test_cfg1_200_steps(cuda):
     assert float(_np(p.f.arr).sum()) == float(G["f_init_sum"])
     p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, 200)
     en = np.asarray(p.stepper.field_energy)
-    err_e = np.max(np.abs(en / G["energy"] - 1))
+    # normwise over the history (the energy dips to 3e-7 of its peak near step 157)
+    err_e = history_err(en, G["energy"])
     assert err_e < 1e-12, err_e
+    # the reference's own spread (8 vs 1 BLAS threads) is of the same order
+    noise = history_err(golden("cfg1_200_blas1")["energy"], G["energy"])
+    assert noise < 1e-12
     np.testing.assert_allclose(p.stepper.time_array, G["time"], rtol=1e-13)
     f = _np(p.f.arr)[INNER]
     assert rel_err(f[:, :, :, :, 7, 3], G["final_slice_xu"]) < F_RTOL

@@ -91,3 +91,13 @@ def test_cfg1_first_steps():
     np.testing.assert_allclose(rec.field_energy, G["energy"][:4], rtol=1e-12)
     np.testing.assert_allclose(rec.dt_history, G["dt"][:4], rtol=1e-14)
     np.testing.assert_allclose(rec.time_array, G["time"][:4], rtol=1e-14)
+
+
+def test_cfg1_reference_noise_floor():
+    """The reference run twice with different BLAS thread counts: its energy histories agree
+    normwise to well below the 1e-12 parity bar (the floor any reimplementation sits on)."""
+    from helpers import history_err
+
+    a, b = golden("cfg1_200"), golden("cfg1_200_blas1")
+    assert history_err(b["energy"], a["energy"]) < 1e-13
+    np.testing.assert_allclose(b["time"], a["time"], rtol=1e-14)
