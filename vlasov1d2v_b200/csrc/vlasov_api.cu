@@ -627,6 +627,7 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     st.E = E;
     st.dt = &state->dt;
     st.state = state;
+    st.err = &state->status;   // bounded-wait timeouts are reported in the loop state
     st.xhalo = VL_XHALO_PERIODIC;
     st.partials = partials;
     for (int it = 0; it < nsteps; ++it) {
