@@ -180,6 +180,23 @@ VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, 
  * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */
 VL_API int vl_sync_ghosts(vl_ctx *ctx, void *f, void *stage, void *stream);
 
+/* ---- the loop without a caller-provided workspace ------------------------------------------- */
+
+/* No counterpart in the reference.  vl_ssp_rk3_steps for callers that cannot allocate device
+ * memory themselves -- e.g. a host recording the loop into a CUDA graph while allocation is
+ * not allowed, a plugin whose host framework owns the whole device heap, or a binding that
+ * holds only raw buffer pointers and a stream.  Same arguments and results as
+ * vl_ssp_rk3_steps minus the workspace: the moment-partial scratch is a file-scope device array
+ * of VL_NOALLOC_SCRATCH_BYTES inside the library (every GPU that loads the library holds it
+ * until the process exits).  Problems whose vl_workspace_bytes exceeds that size are rejected
+ * with VL_ERR_TOO_LARGE.  The first call on a device looks the array's address up with that
+ * device current; make it before any stream capture.  All calls share the array and it keeps
+ * the last call's contents (the loop rewrites what it reads, nothing needs clearing), so calls
+ * whose kernels overlap on the GPU race on it.  Nothing here calls cudaMalloc or cudaFree.     */
+#define VL_NOALLOC_SCRATCH_BYTES (1u << 20)
+VL_API int vl_ssp_rk3_steps_noalloc(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, double *E,
+                                    double *phi, vl_run_state *state, int nsteps, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,7 +24,9 @@ EXPORTED = (
     "vl_ctx_create", "vl_ctx_destroy", "vl_last_error", "vl_abi_version", "vl_state_elems",
     "vl_workspace_bytes", "vl_rhs", "vl_rhs_weighted", "vl_moment", "vl_poisson", "vl_field_energy", "vl_adapt_dt",
     "vl_rk_stage", "vl_run_state_init", "vl_ssp_rk3_steps", "vl_sync_ghosts",
+    "vl_ssp_rk3_steps_noalloc",
 )
+NOALLOC_SCRATCH_BYTES = 1 << 20
 
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 
@@ -93,6 +95,7 @@ def _declare(lib):
                                       ctypes.c_int32, vp, vp]
     lib.vl_ssp_rk3_steps.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i, vp]
     lib.vl_sync_ghosts.argtypes = [vp, vp, vp, vp]
+    lib.vl_ssp_rk3_steps_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp]
     for name in EXPORTED:
         if name not in ("vl_last_error", "vl_abi_version", "vl_state_elems", "vl_workspace_bytes"):
             getattr(lib, name).restype = i

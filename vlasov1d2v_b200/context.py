@@ -188,6 +188,16 @@ class NativeContext:
                   _ptr(state), _ptr(self.workspace), int(nsteps), ctypes.c_void_p(stream_handle()))
 
 
+    def ssp_rk3_steps_noalloc(self, f, sa, sb, E, phi, state, nsteps):
+        """The loop without a workspace argument: its scratch is a fixed device array inside
+        the library (see ``vl_ssp_rk3_steps_noalloc`` in include/vlasov1d2v.h)."""
+        self._check_state(f, "f")
+        self._check_state(sa, "stage_a")
+        self._check_state(sb, "stage_b")
+        _lib.call("vl_ssp_rk3_steps_noalloc", self.handle, _ptr(f), _ptr(sa), _ptr(sb), _ptr(E),
+                  _ptr(phi), _ptr(state), int(nsteps), ctypes.c_void_p(stream_handle()))
+
+
 def get_context(grids, *, precision="fp64", accel=0.0, bfield=0.0, kappa=0.0, courant=1.0):
     """Cached context for a ``Grid3D`` (full phase space) or an x ``Grid1D`` (field-only)."""
     key = (precision, float(accel), float(bfield), float(kappa), float(courant),

@@ -369,6 +369,8 @@ int upload(P **dst, const void *src, size_t bytes) {
 
 }  // namespace
 
+void vl_internal_set_error(const char *msg) { g_err = msg ? msg : ""; }
+
 extern "C" {
 
 const char *vl_last_error(void) { return g_err.c_str(); }
