@@ -115,7 +115,8 @@ VL_API int vl_abi_version(void);
 
 /* number of elements of one ghost-inclusive state array: (nx+2) n (nu+2) n (nv+2) n */
 VL_API size_t vl_state_elems(const vl_ctx *ctx);
-/* bytes of scratch the stepper / moment entry points need (caller allocates, 256-B aligned) */
+/* bytes of scratch vl_ssp_rk3_steps needs (caller allocates, 256-B aligned): the moment
+ * partials of the stage kernels, then the field solve's mode coefficients and ticket counter */
 VL_API size_t vl_workspace_bytes(const vl_ctx *ctx);
 
 /* ---- hot-path operators ------------------------------------------------------------------ */
@@ -137,7 +138,8 @@ VL_API int vl_moment(vl_ctx *ctx, const void *f, double *rho, void *stream);
 
 /* Elliptic.poisson2 (main/elliptic.py:117-145): spectral solve of the charge density
  * (already mean-subtracted by the caller, as main/timestep.py:155 does).  Writes
- * E[(nx+2)][n] (ghosts periodic) and phi[nx][n] (phi may be NULL).                        */
+ * E[(nx+2)][n] (ghosts periodic) and phi[nx][n] (phi may be NULL).  The mode coefficients
+ * pass through a scratch owned by the context: calls on one context must not overlap.      */
 VL_API int vl_poisson(vl_ctx *ctx, const double *charge_density, double *E, double *phi,
                void *stream);
 
@@ -151,8 +153,9 @@ VL_API int vl_adapt_dt(vl_ctx *ctx, const double *E, double *dt, void *stream);
  *   stage 0:  out = in + dt * RHS(in)                       (in is f^n)
  *   stage 1:  out = 3/4 fn + 1/4 in + 1/4 dt RHS(in)
  *   stage 2:  out = 1/3 fn + 2/3 in + 2/3 dt RHS(in)
- * dt is read from device memory (*dt).  Interior of out only.  If rho_partials is not NULL
- * the stage also writes the moment partials of out (consumed by vl_poisson_from_partials). */
+ * dt is read from device memory (*dt).  Interior of out only.  If workspace is not NULL the
+ * stage also writes the moment partials of out (per x element, one partial density row per
+ * CTA; the loop's field solve sums them).                                                    */
 VL_API int vl_rk_stage(vl_ctx *ctx, int stage, const void *in, const void *fn, void *out,
                 const double *E, const double *dt, int xhalo, void *workspace, void *stream);
 
@@ -186,12 +189,13 @@ VL_API int vl_sync_ghosts(vl_ctx *ctx, void *f, void *stage, void *stream);
  * memory themselves -- e.g. a host recording the loop into a CUDA graph while allocation is
  * not allowed, a plugin whose host framework owns the whole device heap, or a binding that
  * holds only raw buffer pointers and a stream.  Same arguments and results as
- * vl_ssp_rk3_steps minus the workspace: the moment-partial scratch is a file-scope device array
+ * vl_ssp_rk3_steps minus the workspace: the loop's scratch is a file-scope device array
  * of VL_NOALLOC_SCRATCH_BYTES inside the library (every GPU that loads the library holds it
  * until the process exits).  Problems whose vl_workspace_bytes exceeds that size are rejected
  * with VL_ERR_TOO_LARGE.  The first call on a device looks the array's address up with that
  * device current; make it before any stream capture.  All calls share the array and it keeps
- * the last call's contents (the loop rewrites what it reads, nothing needs clearing), so calls
+ * the last call's contents (the loop rewrites what it reads; the one word that must start at zero,
+ * the field solve's ticket counter, is cleared on the call's stream at its start), so calls
  * whose kernels overlap on the GPU race on it.  Nothing here calls cudaMalloc or cudaFree.     */
 #define VL_NOALLOC_SCRATCH_BYTES (1u << 20)
 VL_API int vl_ssp_rk3_steps_noalloc(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, double *E,

@@ -26,6 +26,7 @@ struct vl_ctx {
     int device;
     int sm_count;
     int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
+    int moment_grid_g;  // CTAs per x element of the standalone moment kernel
     double up[vl::NMAX * vl::NMAX];
     double xi[vl::NMAX * 2];
     double xw[vl::NMAX];
@@ -37,6 +38,8 @@ struct vl_ctx {
     double2 *d_fwd = nullptr;
     double2 *d_inv = nullptr;
     double *d_tables = nullptr;   // up [n n], xi [n 2], qw [n n]
+    double *d_field = nullptr;    // field scratch of vl_poisson (mode coefficients)
+    double *d_moment = nullptr;   // moment partials of vl_moment [nx][moment_grid_g][n]
     int *d_err = nullptr;         // device error word of operators run without a loop state
     bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
@@ -265,7 +268,8 @@ int launch_moment_t(const vl_ctx *c, const void *f, double *out, int G, cudaStre
     a.nu = c->cfg.nu;
     a.nv = c->cfg.nv;
     for (int i = 0; i < N * N; ++i) a.qw[i] = c->qw[i];
-    vl::moment_kernel<N, T><<<c->cfg.nx * N, 256, 0, s>>>(a);
+    const dim3 grid((unsigned)G, (unsigned)c->cfg.nx);
+    vl::moment_kernel<N, T><<<grid, vl::MOMENT_THREADS, 0, s>>>(a);
     return check_launch("moment_kernel");
 }
 
@@ -317,9 +321,29 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     return a;
 }
 
+// forward DFT over mode slices, then inverse over node slices (a.scratch carries the
+// coefficients between the two)
 int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
-    vl::field_kernel<<<1, vl::FIELD_THREADS, 0, s>>>(a);
-    return check_launch("field_kernel");
+    const int nn = c->cfg.nx * c->cfg.n;
+    const int gf = (c->cfg.n_modes + vl::FWD_MODES - 1) / vl::FWD_MODES;
+    const int gi = (nn + vl::INV_NODES - 1) / vl::INV_NODES;
+    vl::field_fwd_kernel<<<gf, vl::FIELD_THREADS, 0, s>>>(a);
+    int rc = check_launch("field_fwd_kernel");
+    if (rc) return rc;
+    vl::field_inv_kernel<<<gi, vl::FIELD_THREADS, 0, s>>>(a);
+    return check_launch("field_inv_kernel");
+}
+
+// byte offset of the field scratch inside a loop workspace (after the moment partials)
+size_t partials_bytes(const vl_ctx *c) {
+    const int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
+    const size_t b = sizeof(double) * (size_t)c->cfg.nx * g * c->cfg.n;
+    return (b + 255) & ~(size_t)255;
+}
+
+size_t field_scratch_bytes(const vl_ctx *c) {
+    const size_t b = sizeof(double) * vl::field_scratch_doubles(c->cfg.n_modes);
+    return (b + 255) & ~(size_t)255;
 }
 
 vl::ScalarArgs scalar_args(const vl_ctx *c, const double *E) {
@@ -446,6 +470,11 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         c->d_err = e0;
         ee = cudaMemset(c->d_err, 0, sizeof(int));
         if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMemset(err)"));
+        const size_t fb = sizeof(double) * vl::field_scratch_doubles(cfg->n_modes);
+        ee = cudaMalloc((void **)&c->d_field, fb);
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMalloc(field scratch)"));
+        ee = cudaMemset(c->d_field, 0, fb);
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMemset(field scratch)"));
     }
     c->use_tma = (cfg->precision == VL_FP64 ? tma_supported<double>(*cfg) : tma_supported<float>(*cfg)) &&
                  encode_fn() != nullptr;
@@ -464,6 +493,16 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if (g > tiles) g = tiles;
     if (g < 1) g = 1;
     c->stage_grid_g = g;
+    // standalone moment: MOMENT_CTAS_PER_SM resident CTAs per SM, at most one per u element
+    int gm = (c->sm_count * vl::MOMENT_CTAS_PER_SM) / cfg->nx;
+    if (gm > cfg->nu) gm = cfg->nu;
+    if (gm < 1) gm = 1;
+    c->moment_grid_g = gm;
+    {
+        const cudaError_t ee =
+            cudaMalloc((void **)&c->d_moment, sizeof(double) * (size_t)cfg->nx * gm * n);
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMalloc(moment partials)"));
+    }
     *out = c;
     return VL_OK;
 }
@@ -477,6 +516,8 @@ int vl_ctx_destroy(vl_ctx *c) {
     cudaFree(c->d_fwd);
     cudaFree(c->d_inv);
     cudaFree(c->d_tables);
+    cudaFree(c->d_field);
+    cudaFree(c->d_moment);
     cudaFree(c->d_err);
     delete c;
     return VL_OK;
@@ -490,8 +531,7 @@ size_t vl_state_elems(const vl_ctx *c) {
 
 size_t vl_workspace_bytes(const vl_ctx *c) {
     if (c == nullptr) return 0;
-    const size_t b = sizeof(double) * (size_t)c->cfg.nx * c->stage_grid_g * c->cfg.n;
-    return (b + 255) & ~(size_t)255;
+    return partials_bytes(c) + field_scratch_bytes(c);
 }
 
 int vl_rhs(vl_ctx *c, const void *f, const double *E, void *out, int xhalo, void *stream) {
@@ -524,7 +564,13 @@ int vl_rhs_weighted(vl_ctx *c, const void *f, const double *E, void *out, int xh
 
 int vl_moment(vl_ctx *c, const void *f, double *rho, void *stream) {
     if (!c || !f || !rho) return fail(VL_ERR_INVALID, "null argument");
-    return moment(c, f, rho, 1, as_stream(stream));
+    cudaStream_t s = as_stream(stream);
+    const int G = c->moment_grid_g;
+    int rc = moment(c, f, c->d_moment, G, s);
+    if (rc) return rc;
+    const int nn = c->cfg.nx * c->cfg.n;
+    vl::moment_reduce_kernel<<<(nn + 255) / 256, 256, 0, s>>>(c->d_moment, rho, c->cfg.nx, G, c->cfg.n);
+    return check_launch("moment_reduce_kernel");
 }
 
 int vl_poisson(vl_ctx *c, const double *charge, double *E, double *phi, void *stream) {
@@ -533,6 +579,7 @@ int vl_poisson(vl_ctx *c, const double *charge, double *E, double *phi, void *st
     a.charge_in = charge;
     a.E = E;
     a.phi = phi;
+    a.scratch = c->d_field;
     return field(c, a, as_stream(stream));
 }
 
@@ -616,13 +663,17 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     if (nsteps < 0) return fail(VL_ERR_INVALID, "nsteps < 0");
     cudaStream_t s = as_stream(stream);
     double *partials = static_cast<double *>(workspace);
+    double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) + partials_bytes(c));
     const int G = c->stage_grid_g;
     int rc;
+    // the field solve's ticket counter starts at zero (the last CTA of each record resets it)
+    VL_CUDA(cudaMemsetAsync(fscratch + 4 * (size_t)c->cfg.n_modes, 0, sizeof(int), s));
     // moment partials of f^n for the first step's field solve
-    if ((rc = moment(c, f, partials, G, s))) return rc;
+    if ((rc = moment(c, f, partials, c->moment_grid_g, s))) return rc;
     vl::FieldArgs fa = field_args(c);
     fa.partials = partials;
-    fa.G = G;
+    fa.scratch = fscratch;
+    fa.G = c->moment_grid_g;
     fa.E = E;
     fa.state = state;
     vl::StageArgs st = stage_args(c);
@@ -637,6 +688,7 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
         fa.mode = vl::FIELD_PROMOTE;
         fa.phi = nullptr;
         if ((rc = field(c, fa, s))) return rc;
+        fa.G = G;   // from here on the partials come from the stage kernels
         st.in = f;
         st.fn = nullptr;
         st.out = sa;

@@ -88,9 +88,35 @@ __device__ __forceinline__ dd shfl_down_dd(dd v, int off) {
 }
 
 // ----------------------------------------------------------------------------------------------
-// standalone moment: one CTA per (x element e, x node i); writes rho[e][i] at
-// out[(e * G + 0) * N + i] with out[(e * G + g) * N + i] = 0 for g > 0 (partials layout).
+// standalone moment: grid (G, nx).  CTA (g, e) sums the interior u elements
+// [g nu / G, (g + 1) nu / G) of x slab e for every x node i and writes
+// out[(e G + g) n + i] -- the layout of the stage kernels' moment partials.
+// Columns go to threads with a stride that is a multiple of n, so each thread sees one v node
+// k and keeps its row of weights w_j w_k / (J_u J_v) in registers.
 // ----------------------------------------------------------------------------------------------
+// runtime-indexed read of a small register array (unrolled select)
+template <int N>
+__device__ __forceinline__ double acc_at(const double (&v)[N], int i) {
+    double r = v[0];
+#pragma unroll
+    for (int m = 1; m < N; ++m)
+        if (m == i) r = v[m];
+    return r;
+}
+
+// block-wide double-double sum (all threads call); result valid in every thread
+__device__ __forceinline__ double block_sum_dd_rt(double v, double c, dd *scratch) {
+    dd s = {v, c};
+    for (int off = 16; off > 0; off >>= 1) s = dd_add(s, shfl_down_dd(s, off));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) scratch[warp] = s;
+    __syncthreads();
+    dd t = scratch[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = dd_add(t, scratch[w]);
+    return t.hi + t.lo;
+}
+
 struct MomentArgs {
     const void *f;
     double *out;
@@ -99,42 +125,69 @@ struct MomentArgs {
     double qw[NMAX * NMAX];
 };
 
+constexpr int MOMENT_THREADS = 256;
+constexpr int MOMENT_CTAS_PER_SM = 4;
+
 template <int N, typename T>
-__global__ void __launch_bounds__(256) moment_kernel(const MomentArgs a) {
+__global__ void __launch_bounds__(MOMENT_THREADS, MOMENT_CTAS_PER_SM) moment_kernel(const MomentArgs a) {
     const T *__restrict__ f = static_cast<const T *>(a.f);
-    const int e = blockIdx.x / N, i = blockIdx.x % N;
-    const int U = a.nu + 2, V = a.nv + 2;
-    const size_t sJ = (size_t)V * N, sA = sJ * N, sI = sA * U, sE = sI * N;
-    const size_t plane = (size_t)(e + 1) * sE + (size_t)i * sI;
-    const int ncol = a.nv * N;
-    const int nrow = a.nu * N;
-    double acc = 0.0, comp = 0.0;
-    for (int idx = threadIdx.x; idx < nrow * ncol; idx += blockDim.x) {
-        const int r = idx / ncol, c = idx - (idx / ncol) * ncol;
-        const int au = r / N, j = r % N;
-        const int k = c % N;
-        const double v = a.qw[j * N + k] * (double)f[plane + (size_t)(au + 1) * sA + (size_t)j * sJ + N + c];
-        // Neumaier compensated accumulation
-        const double t = acc + v;
-        comp += (fabs(acc) >= fabs(v)) ? ((acc - t) + v) : ((v - t) + acc);
-        acc = t;
+    constexpr int CT = (MOMENT_THREADS / N) * N;   // column threads (stride keeps k fixed)
+    const int g = blockIdx.x, Gn = gridDim.x, e = blockIdx.y;
+    const int nu = a.nu, nv = a.nv;
+    const int U = nu + 2, V = nv + 2;
+    const int sJ = V * N, sA = sJ * N, sI = sA * U;
+    const size_t slab = (size_t)(e + 1) * ((size_t)sI * N);
+    const int a_lo = (int)(((long long)g * nu) / Gn), a_hi = (int)(((long long)(g + 1) * nu) / Gn);
+    const int tid = threadIdx.x;
+    const int ncol = nv * N;
+    const int k = tid % N;
+    double w[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) w[j] = a.qw[j * N + k];
+    double acc[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) acc[i] = 0.0;
+    if (tid < CT) {
+        for (int au = a_lo; au < a_hi; ++au) {
+            const T *pa = f + slab + (size_t)(au + 1) * sA + N;   // interior columns start at N
+            for (int c = tid; c < ncol; c += CT) {
+#pragma unroll
+                for (int i = 0; i < N; ++i) {
+                    double s = 0.0;
+#pragma unroll
+                    for (int j = 0; j < N; ++j) s = fma(w[j], (double)pa[(size_t)i * sI + j * sJ + c], s);
+                    acc[i] += s;
+                }
+            }
+        }
     }
-    dd s = {acc, comp};
-    for (int off = 16; off > 0; off >>= 1) s = dd_add(s, shfl_down_dd(s, off));
-    __shared__ dd red[32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) red[warp] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        dd t = red[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = dd_add(t, red[w]);
-        a.out[((size_t)e * a.G) * N + i] = t.hi + t.lo;
-        for (int gg = 1; gg < a.G; ++gg) a.out[((size_t)e * a.G + gg) * N + i] = 0.0;
+    __shared__ dd red[MOMENT_THREADS / 32];
+    for (int i = 0; i < N; ++i) {
+        const double tot = block_sum_dd_rt(acc_at(acc, i), 0.0, red);
+        if (tid == 0) a.out[((size_t)e * Gn + g) * N + i] = tot;
     }
 }
 
+// rho[e][i] = sum over g of the partials [e][g][i] (double-double, fixed order)
+__global__ void moment_reduce_kernel(const double *__restrict__ partials, double *__restrict__ rho,
+                                     int nx, int G, int n) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nx * n) return;
+    const int e = p / n, i = p - e * n;
+    dd s = {0.0, 0.0};
+    for (int g = 0; g < G; ++g) s = dd_add(s, dd{partials[((size_t)e * G + g) * n + i], 0.0});
+    rho[p] = s.hi + s.lo;
+}
+
 // ----------------------------------------------------------------------------------------------
-// field kernel (single CTA)
+// field solve: two multi-CTA kernels
+//   field_fwd_kernel  every CTA forms the charge kappa (mean rho - rho) from the moment partials
+//                     (fixed summation order), then a slice of FWD_MODES modes:
+//                     c_m = (sum_{e,j} rhs T[e,j,m]) dx / L, Ehat_m = -c_m/(i k_m),
+//                     phihat_m = -c_m / k_m^2 (k = 0 mode dropped) -> scratch
+//   field_inv_kernel  a slice of INV_NODES nodes: E = Re sum_m Ehat_m P[m,e,j], phi likewise,
+//                     periodic ghost rows.  After stage 2 the last CTA to finish (ticket
+//                     counter) records the energy, adapts dt and updates the loop state.
 // ----------------------------------------------------------------------------------------------
 enum FieldMode : int {
     FIELD_REQUIRE_ACTIVE = 1,  // return if !state->active
@@ -150,6 +203,7 @@ struct FieldArgs {
     double *phi;              // [nx n] or null
     vl_run_state *state;      // or null
     int mode;
+    double *scratch;          // [4 M] Ehat | phihat (complex, interleaved), then an int counter
     const double2 *fwd;       // [nx n][M]
     const double2 *inv;       // [M][nx n]
     const double *k;          // [M]
@@ -158,24 +212,17 @@ struct FieldArgs {
     double kappa, dx, length, accel, bfield, umax, vmax, du, dv, courant;
 };
 
-constexpr int FIELD_THREADS = 512;
+constexpr int FIELD_THREADS = 1024;
+constexpr int FWD_MODES = 16;                  // modes per forward CTA
+constexpr int INV_NODES = 16;                  // nodes per inverse CTA
+constexpr int FIELD_PARTS = FIELD_THREADS / 16;   // partial sums per mode / node
 constexpr int FIELD_MAX_NODES = 64 * NMAX;    // nx * n capacity of the shared buffers
 constexpr int FIELD_MAX_MODES = 2 * 160 + 1;  // M capacity
 
+__host__ __device__ constexpr size_t field_scratch_doubles(int M) { return 4 * (size_t)M + 8; }
+
 __device__ __forceinline__ double block_sum_dd(double v, double c, dd *scratch) {
-    dd s = {v, c};
-    for (int off = 16; off > 0; off >>= 1) s = dd_add(s, shfl_down_dd(s, off));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) scratch[warp] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        dd t = scratch[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = dd_add(t, scratch[w]);
-        scratch[0] = t;
-    }
-    __syncthreads();
-    return scratch[0].hi + scratch[0].lo;
+    return block_sum_dd_rt(v, c, scratch);
 }
 
 __device__ __forceinline__ double block_max(double v, double *scratch) {
@@ -184,55 +231,48 @@ __device__ __forceinline__ double block_max(double v, double *scratch) {
     __syncthreads();
     if (lane == 0) scratch[warp] = v;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = scratch[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = fmax(t, scratch[w]);
-        scratch[0] = t;
-    }
-    __syncthreads();
-    return scratch[0];
+    double t = scratch[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) t = fmax(t, scratch[w]);
+    return t;
 }
 
-__global__ void __launch_bounds__(FIELD_THREADS) field_kernel(const FieldArgs a) {
-    __shared__ double s_rhs[FIELD_MAX_NODES];
-    __shared__ double2 s_E[FIELD_MAX_MODES];
-    __shared__ double2 s_P[FIELD_MAX_MODES];
-    __shared__ dd s_red[FIELD_THREADS / 32];
-    __shared__ double s_max[FIELD_THREADS / 32];
-    __shared__ int s_flag;
-
+// returns false when this step is inactive (all threads agree)
+__device__ __forceinline__ bool field_gate(const FieldArgs &a, bool first_cta) {
     vl_run_state *st = a.state;
-    const int tid = threadIdx.x;
-    if (st != nullptr) {
-        if (a.mode & FIELD_PROMOTE) {
-            const int go = st->active_next;
-            __syncthreads();
-            if (tid == 0) {
-                st->active = go;
-                if (go) st->dt = st->dt_next;
-            }
-            if (!go) return;
-        } else if (a.mode & FIELD_REQUIRE_ACTIVE) {
-            if (st->active == 0) return;
+    if (st == nullptr) return true;
+    if (a.mode & FIELD_PROMOTE) {
+        const int go = st->active_next;
+        if (first_cta && threadIdx.x == 0) {
+            st->active = go;
+            if (go) st->dt = st->dt_next;
         }
+        return go != 0;
     }
+    if (a.mode & FIELD_REQUIRE_ACTIVE) return st->active != 0;
+    return true;
+}
+
+__global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArgs a) {
+    __shared__ double s_rhs[FIELD_MAX_NODES];
+    __shared__ double s_cr[FIELD_PARTS][FWD_MODES + 1], s_ci[FIELD_PARTS][FWD_MODES + 1];
+    __shared__ dd s_red[FIELD_THREADS / 32];
+    static_assert(FIELD_PARTS * FWD_MODES == FIELD_THREADS && FIELD_PARTS == 64 &&
+                      FWD_MODES <= FIELD_THREADS / 32, "forward thread layout");
+    if (!field_gate(a, blockIdx.x == 0)) return;
+    const int tid = threadIdx.x;
     const int nn = a.nx * a.n;
     const int M = a.M;
-
-    // ---- density and charge ----
-    double loc = 0.0, locc = 0.0;
     if (a.charge_in != nullptr) {
         for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * a.charge_in[p];
         __syncthreads();
     } else {
+        double loc = 0.0, locc = 0.0;
         for (int p = tid; p < nn; p += blockDim.x) {
             const int e = p / a.n, i = p - (p / a.n) * a.n;
-            dd s = {0.0, 0.0};
-            for (int gg = 0; gg < a.G; ++gg) {
-                const double v = a.partials[((size_t)e * a.G + gg) * a.n + i];
-                s = dd_add(s, dd{v, 0.0});
-            }
-            const double rho = s.hi + s.lo;
+            dd sacc = {0.0, 0.0};
+            for (int gg = 0; gg < a.G; ++gg)
+                sacc = dd_add(sacc, dd{a.partials[((size_t)e * a.G + gg) * a.n + i], 0.0});
+            const double rho = sacc.hi + sacc.lo;
             s_rhs[p] = rho;
             const double t = loc + rho;
             locc += (fabs(loc) >= fabs(rho)) ? ((loc - t) + rho) : ((rho - t) + loc);
@@ -240,22 +280,40 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_kernel(const FieldArgs a)
         }
         const double total = block_sum_dd(loc, locc, s_red);
         const double mean = total / (double)nn;
+        __syncthreads();
         for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * (mean - s_rhs[p]);
         __syncthreads();
     }
-
-    // ---- forward high-order DFT: c_m = (sum_{e,j} rhs T[e,j,m]) dx / L (main/grid.py:78-82) ----
-    const double scale_dx = a.dx, scale_L = a.length;
-    for (int m = tid; m < M; m += blockDim.x) {
-        double cr = 0.0, ci = 0.0;
-        for (int p = 0; p < nn; ++p) {
+    // this CTA's modes: thread (mode slot ml, part) sums nodes p = part, part + PARTS, ...
+    const int ml = tid % FWD_MODES, part = tid / FWD_MODES;
+    const int m = blockIdx.x * FWD_MODES + ml;
+    double cr = 0.0, ci = 0.0;
+    if (m < M) {
+#pragma unroll 4
+        for (int p = part; p < nn; p += FIELD_PARTS) {
             const double2 t = a.fwd[(size_t)p * M + m];
             const double r = s_rhs[p];
             cr = fma(r, t.x, cr);
             ci = fma(r, t.y, ci);
         }
-        cr = (cr * scale_dx) / scale_L;
-        ci = (ci * scale_dx) / scale_L;
+    }
+    s_cr[part][ml] = cr;
+    s_ci[part][ml] = ci;
+    __syncthreads();
+    // warp w folds the 64 partial sums of mode slot w
+    const int w = tid >> 5, lane = tid & 31;
+    const int mw = blockIdx.x * FWD_MODES + w;
+    if (w < FWD_MODES && mw < M) {
+        double sr = s_cr[lane][w] + s_cr[lane + 32][w];
+        double si = s_ci[lane][w] + s_ci[lane + 32][w];
+        for (int off = 16; off > 0; off >>= 1) {
+            sr += __shfl_down_sync(0xffffffffu, sr, off);
+            si += __shfl_down_sync(0xffffffffu, si, off);
+        }
+        if (lane != 0) return;
+        const int m = mw;
+        sr = (sr * a.dx) / a.length;
+        si = (si * a.dx) / a.length;
         const double km = a.k[m];
         double2 Eh, Ph;
         if (km == 0.0) {
@@ -265,21 +323,42 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_kernel(const FieldArgs a)
             Ph = make_double2(0.0, 0.0);
         } else {
             // -(c / (1j k)) = (-c_i / k) + 1j (c_r / k);  -(c / k^2)
-            Eh = make_double2(-(ci / km), cr / km);
+            Eh = make_double2(-(si / km), sr / km);
             const double k2 = km * km;
-            Ph = make_double2(-(cr / k2), -(ci / k2));
+            Ph = make_double2(-(sr / k2), -(si / k2));
         }
-        s_E[m] = Eh;
-        s_P[m] = Ph;
+        double2 *sc = reinterpret_cast<double2 *>(a.scratch);
+        sc[m] = Eh;
+        sc[M + m] = Ph;
+    }
+}
+
+__global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArgs a) {
+    __shared__ double2 s_E[FIELD_MAX_MODES];
+    __shared__ double2 s_P[FIELD_MAX_MODES];
+    __shared__ double s_er[FIELD_PARTS][INV_NODES + 1], s_pr[FIELD_PARTS][INV_NODES + 1];
+    __shared__ dd s_red[FIELD_THREADS / 32];
+    __shared__ double s_max[FIELD_THREADS / 32];
+    __shared__ int s_last;
+    static_assert(FIELD_PARTS * INV_NODES == FIELD_THREADS && FIELD_PARTS == 64 &&
+                      INV_NODES <= FIELD_THREADS / 32, "inverse thread layout");
+    vl_run_state *st = a.state;
+    if (st != nullptr && (a.mode & (FIELD_REQUIRE_ACTIVE | FIELD_PROMOTE)) && st->active == 0) return;
+    const int tid = threadIdx.x;
+    const int nn = a.nx * a.n;
+    const int M = a.M;
+    const double2 *sc = reinterpret_cast<const double2 *>(a.scratch);
+    for (int m = tid; m < M; m += blockDim.x) {
+        s_E[m] = sc[m];
+        s_P[m] = sc[M + m];
     }
     __syncthreads();
-
-    // ---- inverse: E[e,j] = Re sum_m Eh_m P[m,e,j]  (main/grid.py:84-88) ----
-    double esq = 0.0, esqc = 0.0, emax = 0.0;
-    bool bad = false;
-    for (int p = tid; p < nn; p += blockDim.x) {
-        double er = 0.0, pr = 0.0;
-        for (int m = 0; m < M; ++m) {
+    const int nl = tid % INV_NODES, part = tid / INV_NODES;
+    const int p = blockIdx.x * INV_NODES + nl;
+    double er = 0.0, pr = 0.0;
+    if (p < nn) {
+#pragma unroll 4
+        for (int m = part; m < M; m += FIELD_PARTS) {
             const double2 ph = a.inv[(size_t)m * nn + p];
             const double2 eh = s_E[m];
             const double2 qh = s_P[m];
@@ -288,28 +367,53 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_kernel(const FieldArgs a)
             pr = fma(qh.x, ph.x, pr);
             pr = fma(-qh.y, ph.y, pr);
         }
-        a.E[a.n + p] = er;
-        if (p >= nn - a.n) a.E[p - (nn - a.n)] = er;           // E[0] = E[-2]
-        if (p < a.n) a.E[nn + a.n + p] = er;                   // E[-1] = E[1]
-        if (a.phi != nullptr) a.phi[p] = pr;
-        const int j = p % a.n;
-        const double v = a.xw[j] * (er * er);
+    }
+    s_er[part][nl] = er;
+    s_pr[part][nl] = pr;
+    __syncthreads();
+    // warp w folds the 64 partial sums of node slot w
+    const int w = tid >> 5, lane = tid & 31;
+    const int pw = blockIdx.x * INV_NODES + w;
+    if (w < INV_NODES && pw < nn) {
+        double se = s_er[lane][w] + s_er[lane + 32][w];
+        double sp = s_pr[lane][w] + s_pr[lane + 32][w];
+        for (int off = 16; off > 0; off >>= 1) {
+            se += __shfl_down_sync(0xffffffffu, se, off);
+            sp += __shfl_down_sync(0xffffffffu, sp, off);
+        }
+        if (lane == 0) {
+            a.E[a.n + pw] = se;
+            if (pw >= nn - a.n) a.E[pw - (nn - a.n)] = se;   // E[0] = E[-2]
+            if (pw < a.n) a.E[nn + a.n + pw] = se;           // E[-1] = E[1]
+            if (a.phi != nullptr) a.phi[pw] = sp;
+            if (st != nullptr && !isfinite(se)) atomicOr(&st->status, 1);
+        }
+    }
+    if (st == nullptr || !(a.mode & FIELD_RECORD)) return;
+    // ---- last CTA: energy, dt, loop bookkeeping (main/timestep.py:98-103, :184-185) ----
+    int *counter = reinterpret_cast<int *>(a.scratch + 4 * (size_t)M);
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double esq = 0.0, esqc = 0.0, emax = 0.0;
+    bool bad = false;
+    for (int q = tid; q < nn; q += blockDim.x) {
+        const double ev = *((volatile double *)&a.E[a.n + q]);
+        const double v = a.xw[q % a.n] * (ev * ev);
         const double t = esq + v;
         esqc += (fabs(esq) >= fabs(v)) ? ((esq - t) + v) : ((v - t) + esq);
         esq = t;
-        emax = fmax(emax, fabs(a.accel * er));
-        bad |= !isfinite(er);
+        emax = fmax(emax, fabs(a.accel * ev));
+        bad |= !isfinite(ev);
     }
-    if (st == nullptr || !(a.mode & FIELD_RECORD)) {
-        if (st != nullptr && bad) atomicOr(&st->status, 1);
-        return;
-    }
-    if (tid == 0) s_flag = 0;
-    __syncthreads();
-    if (bad) atomicOr(&s_flag, 1);
     const double energy = 0.5 * block_sum_dd(esq, esqc, s_red);
     const double maxE = block_max(emax, s_max);
+    const int any_bad = __syncthreads_or(bad ? 1 : 0);
     if (tid == 0) {
+        *counter = 0;
         // get_max_speeds + adapt_time_step (main/timestep.py:231-242)
         const double ab = a.accel * a.bfield;
         const double s0 = fabs(a.umax);
@@ -328,7 +432,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_kernel(const FieldArgs a)
             if (st->time_hist) st->time_hist[slot] = time;
             if (st->dt_hist) st->dt_hist[slot] = dtn;
         }
-        const bool finite = isfinite(energy) && isfinite(dtn) && (s_flag == 0);
+        const bool finite = isfinite(energy) && isfinite(dtn) && !any_bad;
         if (!finite) st->status |= 1;
         st->active_next = (time < st->final_time) && (steps < st->max_steps) && finite;
     }

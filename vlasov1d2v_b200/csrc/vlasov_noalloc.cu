@@ -1,5 +1,6 @@
-// SSP-RK3 loop entry point that allocates nothing: the moment-partial scratch lives in a
-// file-scope device array instead of a caller-provided workspace.
+// SSP-RK3 loop entry point that allocates nothing: the loop's scratch (moment partials, field
+// mode coefficients, ticket counter) lives in a file-scope device array instead of a
+// caller-provided workspace.
 //
 // Some callers cannot allocate device memory themselves: a host that records the loop into a
 // CUDA graph while allocations are forbidden, a plugin whose host framework owns the whole
@@ -12,8 +13,9 @@
 //   * its device address is looked up once per device with cudaGetSymbolAddress, on the first
 //     call made with that device current (make that first call outside any stream capture);
 //   * all calls share it and it keeps the last call's contents; the loop rewrites every entry
-//     it reads before reading it, so nothing needs clearing, but calls whose kernels overlap on
-//     the GPU (different streams, different contexts) race on it.
+//     it reads before reading it, and the one word that must start at zero (the field solve's
+//     ticket counter) is cleared by vl_ssp_rk3_steps on the call's stream; calls whose kernels
+//     overlap on the GPU (different streams, different contexts) race on it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -46,7 +48,7 @@ VL_API int vl_ssp_rk3_steps_noalloc(vl_ctx *ctx, void *f, void *stage_a, void *s
     }
     const size_t need = vl_workspace_bytes(ctx);
     if (need > (size_t)VL_NOALLOC_SCRATCH_BYTES) {
-        const std::string msg = "vl_ssp_rk3_steps_noalloc: the moment scratch of this problem needs " +
+        const std::string msg = "vl_ssp_rk3_steps_noalloc: the loop scratch of this problem needs " +
                                 std::to_string(need) + " bytes, above the fixed " +
                                 std::to_string((size_t)VL_NOALLOC_SCRATCH_BYTES) +
                                 "-byte capacity; use vl_ssp_rk3_steps with a workspace";
