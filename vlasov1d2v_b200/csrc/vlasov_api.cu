@@ -20,6 +20,7 @@
 #include "vlasov_kernels.cuh"
 #include "vlasov_stage.cuh"
 #include "vlasov_stage_tma.cuh"
+#include "vlasov_stage_frag.cuh"
 
 struct vl_ctx {
     vl_config cfg;      // scalars (pointer members cleared)
@@ -42,6 +43,7 @@ struct vl_ctx {
     double *d_moment = nullptr;   // moment partials of vl_moment [nx][moment_grid_g][n]
     int *d_err = nullptr;         // device error word of operators run without a loop state
     bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
+    bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
 };
 
@@ -111,7 +113,11 @@ int state_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     cuuint64_t dims[5] = {V * N, (cuuint64_t)N, U, (cuuint64_t)N, X};
     cuuint64_t strides[4] = {V * N * es, V * N * N * es, V * N * N * U * es, V * N * N * U * N * es};
     cuuint32_t box[5];
+    using F = vl::FragGeom<T>;
     switch (which) {
+        // fragment kernel tiles: one zero-filled row past the j extent pads the plane stride
+        case 6: box[0] = F::W; box[1] = F::ROWS; box[2] = 1; box[3] = N; box[4] = 1; break;
+        case 7: box[0] = F::WF; box[1] = F::ROWS; box[2] = 1; box[3] = N; box[4] = 1; break;
         case 0: case 5: box[0] = G::W; box[1] = N; box[2] = 1; box[3] = N; box[4] = 1; break;
         case 1: box[0] = G::COLS; box[1] = N; box[2] = 1; box[3] = 1; box[4] = 1; break;
         case 2: box[0] = G::COLS; box[1] = 1; box[2] = 1; box[3] = N; box[4] = 1; break;
@@ -140,6 +146,10 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     for (int i = 0; i < N * N; ++i) tb.up[i] = (T)c->up[i];
     for (int i = 0; i < 2 * N; ++i) tb.xi[i] = (T)c->xi[i];
     for (int i = 0; i < N * N; ++i) tb.qw[i] = c->qw[i];
+    for (int i = 0; i < N; ++i) {
+        tb.wu[i] = c->xw[i] / c->cfg.ju;
+        tb.wv[i] = c->xw[i] / c->cfg.jv;
+    }
     for (int i = 0; i < N; ++i)
         for (int m = 0; m < N; ++m) {
             double p = c->up[i * N + m], q = c->up[i * N + m];
@@ -151,6 +161,19 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageArgs a = a0;
     if (a.err == nullptr) a.err = c->d_err;
     dim3 grid(c->stage_grid_g, c->cfg.nx);
+    if constexpr (N == 8) {
+        if (c->use_frag) {
+            using G = vl::FragGeom<T>;
+            vl::FragMaps maps;
+            int rc;
+            if ((rc = state_map<N, T>(c, a.in, 6, &maps.in_tile))) return rc;
+            if ((rc = state_map<N, T>(c, a.in, 1, &maps.in_xface))) return rc;
+            if ((rc = state_map<N, T>(c, a.in, 2, &maps.in_uface))) return rc;
+            if ((rc = state_map<N, T>(c, a.fn ? a.fn : a.in, 7, &maps.fn_tile))) return rc;
+            vl::stage_frag_kernel<T><<<grid, G::THREADS, G::smem_bytes(), s>>>(a, tb, maps);
+            return check_launch("stage_frag_kernel");
+        }
+    }
     if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
         if (c->use_tma) {
             using G = vl::TmaGeom<N, T>;
@@ -192,8 +215,20 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma) {
+int stage_occupancy_t(bool tma, bool frag) {
     int blocks = 0;
+    if constexpr (N == 8) {
+        if (frag) {
+            using G = vl::FragGeom<T>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_frag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T>,
+                                                              G::THREADS, smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
+    }
     if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
         if (tma) {
             using G = vl::TmaGeom<N, T>;
@@ -225,18 +260,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma) {
+int stage_occupancy(int n, bool tma, bool frag) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma);
-        case 2: return stage_occupancy_t<2, T>(tma);
-        case 3: return stage_occupancy_t<3, T>(tma);
-        case 4: return stage_occupancy_t<4, T>(tma);
-        case 5: return stage_occupancy_t<5, T>(tma);
-        case 6: return stage_occupancy_t<6, T>(tma);
-        case 7: return stage_occupancy_t<7, T>(tma);
-        case 8: return stage_occupancy_t<8, T>(tma);
-        case 9: return stage_occupancy_t<9, T>(tma);
-        case 10: return stage_occupancy_t<10, T>(tma);
+        case 1: return stage_occupancy_t<1, T>(tma, frag);
+        case 2: return stage_occupancy_t<2, T>(tma, frag);
+        case 3: return stage_occupancy_t<3, T>(tma, frag);
+        case 4: return stage_occupancy_t<4, T>(tma, frag);
+        case 5: return stage_occupancy_t<5, T>(tma, frag);
+        case 6: return stage_occupancy_t<6, T>(tma, frag);
+        case 7: return stage_occupancy_t<7, T>(tma, frag);
+        case 8: return stage_occupancy_t<8, T>(tma, frag);
+        case 9: return stage_occupancy_t<9, T>(tma, frag);
+        case 10: return stage_occupancy_t<10, T>(tma, frag);
         default: return 1;
     }
 }
@@ -252,7 +287,7 @@ bool tma_supported(const vl_config &g) {
 }
 
 // v elements per tile of the stage kernel
-int stage_epw(int n) { return 32 / n; }
+int stage_epw(int n) { return 32 / n; }   // 4 at n = 8 for both the TMA and fragment kernels
 
 // ------------------------------------------------------------------------------------------
 // moment kernel dispatch
@@ -483,8 +518,13 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         if (env && env[0] == '1') c->use_tma = false;
     }
     // CTAs per x element: fill the device (resident CTAs x SMs), at most one per tile
-    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma)
-                                              : stage_occupancy<float>(n, c->use_tma);
+    c->use_frag = c->use_tma && n == 8;
+    {
+        const char *env = getenv("VLASOV1D2V_NO_FRAG");
+        if (env && env[0] == '1') c->use_frag = false;
+    }
+    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma, c->use_frag)
+                                              : stage_occupancy<float>(n, c->use_tma, c->use_frag);
     const int bt = stage_epw(n);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double

@@ -37,6 +37,9 @@ struct StageTables {
     //   speed <  0: d = sum_m upM[i][m] f[m] - xi[i][1] * (right neighbour trace)
     T upP[NMAX * NMAX];
     T upM[NMAX * NMAX];
+    // the velocity weights factored: w_j w_k / (J_u J_v) = (w_j / J_u) (w_k / J_v)
+    double wu[NMAX];
+    double wv[NMAX];
 };
 
 struct StageArgs {

@@ -1,0 +1,353 @@
+// Fused SSP-RK stage kernel for n = 8 in the quad-fragment layout (sm_100a).
+//
+// Tile = (x element e, u element a, 4 consecutive v elements): 32 v-node columns, 8 x 8 (i, j)
+// rows.  Warp w owns v element w of the tile; inside a warp, lane = 4 g + t owns the two
+// output columns k = 2t, 2t + 1 of x node i = g, for all eight j.  That is the accumulator
+// layout of the FP64 tensor-core instruction mma.m8n8k4 (D[g][2t..2t+1]), so per j the
+// x and v contractions run on the tensor cores (FP64 form) and land directly in the thread's
+// outputs:
+//   x:  D[i][k] += sum_m up[i][m] F[m][j][k]       A = up (registers), B = tile plane rows
+//   v:  D[i][k] += sum_m F[i][j][m] up[k][m]       A = tile row slice, B = up^T (registers)
+// with the upwind lifts as a third k-chunk of each (two nonzero columns).  The u contraction
+// mixes the j of one thread's own outputs and runs on the FMA pipes from a per-thread copy of
+// F[i][0..7][k..k+1].  The FP32 form runs all three contractions on the FMA pipes in the
+// same layout.
+//
+// Shared-memory stage (one TMA box each, no multicast):
+//   IN [i][9][36 | 40]   stage input incl. pad columns (v traces) and one zero-filled row:
+//                        the plane stride 9 W is 8 banks mod 32, so the fragment loads of
+//                        four or eight planes are conflict-free
+//   FN [i][9][34 | 36]   f^n (combination stages only)
+//   XF [side][j][32]     x upwind traces: (e-1, i = n-1) and (e+1, i = 0)
+//   UF [side][i][32]     u upwind traces: (a-1, j = n-1) and (a+1, j = 0)
+// Two stages: tile q+1 streams in while tile q is computed.  Every wait is bounded: on timeout
+// the kernel raises bit 1 of the error word and returns.
+#pragma once
+
+#include <cuda.h>
+
+#include "vlasov_kernels.cuh"
+#include "vlasov_stage.cuh"
+#include "vlasov_stage_tma.cuh"
+
+namespace vl {
+
+template <typename T>
+struct FragGeom {
+    static constexpr int N = 8;
+    static constexpr int EPT = 4;                    // v elements per tile (one per warp)
+    static constexpr int COLS = EPT * N;             // 32
+    static constexpr int P = 16 / (int)sizeof(T);    // pad columns each side of IN (16 bytes)
+    static constexpr int W = COLS + 2 * P;           // IN row length: 36 (FP64) | 40 (FP32)
+    static constexpr int ROWS = N + 1;               // j rows per plane incl. one fill row
+    static constexpr int PS = W * ROWS;              // IN plane stride: 324 | 360
+    static constexpr int WF = COLS + P;              // FN row length: 34 | 36
+    static constexpr int PSF = WF * ROWS;            // FN plane stride: 306 | 324
+    static constexpr int THREADS = 32 * EPT;
+    static constexpr bool MMA = sizeof(T) == 8;      // tensor-core x/v contractions (FP64)
+    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
+    static constexpr size_t IN_B = al(sizeof(T) * (size_t)PS * N);
+    static constexpr size_t FN_B = al(sizeof(T) * (size_t)PSF * N);
+    static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * COLS * N);
+    static constexpr size_t UF_B = XF_B;
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B;
+    static constexpr size_t smem_bytes() { return 2 * STAGE_B + 128; }
+    static constexpr uint32_t TX_IN = sizeof(T) * W * ROWS * N;
+    static constexpr uint32_t TX_FN = sizeof(T) * WF * ROWS * N;
+    static constexpr uint32_t TX_FACE = sizeof(T) * COLS * N;
+};
+
+struct FragMaps {
+    CUtensorMap in_tile;   // box (W, 9, 1, n, 1) over the stage input
+    CUtensorMap in_xface;  // box (32, n, 1, 1, 1)
+    CUtensorMap in_uface;  // box (32, 1, 1, n, 1)
+    CUtensorMap fn_tile;   // box (WF, 9, 1, n, 1) over f^n
+};
+
+// D[8x8] += A[8x4] B[4x8] in FP64 on the tensor cores; per lane (g = lane/4, t = lane%4):
+// a = A[g][t], b = B[t][g], d0/d1 = D[g][2t], D[g][2t+1]
+__device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
+}
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+    using V = double2;
+};
+template <>
+struct Pair<float> {
+    using V = float2;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(FragGeom<T>::THREADS, 2)
+stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
+                  const __grid_constant__ FragMaps maps) {
+    using G = FragGeom<T>;
+    using V2 = typename Pair<T>::V;
+    constexpr int N = G::N, P = G::P, W = G::W, PS = G::PS, WF = G::WF, PSF = G::PSF;
+    constexpr int COLS = G::COLS, EPT = G::EPT, NT = G::THREADS;
+    if (a.state != nullptr && a.state->active == 0) return;
+
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
+    __shared__ __align__(8) uint64_t full[2];
+    __shared__ dd sRed[EPT][N];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int w = tid >> 5;          // v element of the tile
+    const int g = lane >> 2;         // x node i of the thread's outputs
+    const int t = lane & 3;          // columns 2t, 2t + 1 of the element
+    const int wc = w * N;            // first tile column of the element
+    const int cl = wc + 2 * t;       // first tile column of the thread
+
+    const int nx = a.nx, nu = a.nu, nv = a.nv;
+    const int U = nu + 2, V = nv + 2;
+    const int sJ = V * N, sA = sJ * N, sI = sA * U;
+    const size_t sE_ = (size_t)sI * N;
+    const int e = blockIdx.y, Eg = e + 1;
+    int El, Er;
+    if (a.xhalo == VL_XHALO_PERIODIC) {
+        El = (e == 0) ? nx : e;
+        Er = (e == nx - 1) ? 1 : e + 2;
+    } else {
+        El = e;
+        Er = e + 2;
+    }
+    const int kind = a.kind;
+    const bool with_fn = (kind == KIND_COMBINE);
+    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0);
+    const int nbt = (nv + EPT - 1) / EPT;
+    const int tiles = nu * nbt;
+    const int ntile_cta = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    if (tid == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto stage_ptr = [&](int s) { return base + (size_t)s * G::STAGE_B; };
+    auto issue = [&](int s, int q) {
+        const int tt = blockIdx.x + q * gridDim.x;
+        const int au = tt / nbt;
+        const int b0 = (tt - au * nbt) * EPT;
+        const int Ag = au + 1;
+        const int x0 = (b0 + 1) * N;
+        unsigned char *st = stage_ptr(s);
+        unsigned char *xf = st + G::IN_B + G::FN_B;
+        unsigned char *uf = xf + G::XF_B;
+        mbar_arrive_expect_tx(&full[s], tx_bytes);
+        tma_load_5d(st, &maps.in_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
+        tma_load_5d(xf, &maps.in_xface, &full[s], x0, 0, Ag, N - 1, El);
+        tma_load_5d(xf + sizeof(T) * COLS * N, &maps.in_xface, &full[s], x0, 0, Ag, 0, Er);
+        tma_load_5d(uf, &maps.in_uface, &full[s], x0, N - 1, Ag - 1, 0, Eg);
+        tma_load_5d(uf + sizeof(T) * COLS * N, &maps.in_uface, &full[s], x0, 0, Ag + 1, 0, Eg);
+        if (with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
+    };
+    if (tid == 0) {
+        if (ntile_cta > 0) issue(0, 0);
+        if (ntile_cta > 1) issue(1, 1);
+    }
+
+    const double accel = a.accel, bfield = a.bfield, nbfield = -a.bfield;
+    const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
+    const T dtT = (T)dtd, c0 = (T)a.c0, c1 = (T)a.c1, c2dt = (T)(a.c2 * dtd);
+    const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
+    const double Ei = a.E[Eg * N + g];
+    // per-thread coefficients (runtime rows g and 2t, 2t + 1 of the tables)
+    T ca0, ca1, calift;            // MMA: up[g][t], up[g][4 + t], lift column t of row g
+    T upi[N], upk0[N], upk1[N];    // FMA form: up[g][.], up[2t][.], up[2t + 1][.]
+    T xig0, xig1, xik00, xik01, xik10, xik11;
+    if constexpr (G::MMA) {
+        ca0 = tb.up[g * N + t];
+        ca1 = tb.up[g * N + 4 + t];
+        calift = (t == 0) ? tb.xi[2 * g] : ((t == 1) ? -tb.xi[2 * g + 1] : (T)0);
+    } else {
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            upi[m] = tb.up[g * N + m];
+            upk0[m] = tb.up[(2 * t) * N + m];
+            upk1[m] = tb.up[(2 * t + 1) * N + m];
+        }
+        xig0 = tb.xi[2 * g];
+        xig1 = tb.xi[2 * g + 1];
+        xik00 = tb.xi[4 * t];
+        xik01 = tb.xi[4 * t + 1];
+        xik10 = tb.xi[4 * t + 2];
+        xik11 = tb.xi[4 * t + 3];
+    }
+    T *out = static_cast<T *>(a.out);
+    T *gout = static_cast<T *>(a.ghost_out);
+    double mk0 = 0.0, mk1 = 0.0;   // sum_j (w_j / J_u) out[.., j, k] for the two columns
+
+    for (int q = 0; q < ntile_cta; ++q) {
+        const int s = q & 1;
+        const int tt = blockIdx.x + q * gridDim.x;
+        const int au = tt / nbt;
+        const int b0 = (tt - au * nbt) * EPT;
+        const int nb = min(EPT, nv - b0);
+        const int Ag = au + 1;
+        if (!mbar_wait_bounded(&full[s], (uint32_t)((q >> 1) & 1))) {
+            if (a.err != nullptr) atomicOr(a.err, 2);
+            return;
+        }
+        const T *sIn = reinterpret_cast<const T *>(stage_ptr(s));
+        const T *sFn = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B);
+        const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
+        const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
+
+        if (w < nb) {
+            const int col = (b0 + 1) * N + cl;   // global v-node column of the first output
+            const double sd0 = accel * (Ei + bfield * a.v_nodes[col]);
+            const double sd1 = accel * (Ei + bfield * a.v_nodes[col + 1]);
+            const T sp0 = (T)sd0, sp1 = (T)sd1;
+            // F[g][m][cl..cl+1] for the u contraction, and the u upwind traces
+            const T *pg = sIn + g * PS + P + cl;
+            V2 fu[N];
+#pragma unroll
+            for (int m = 0; m < N; ++m) fu[m] = *reinterpret_cast<const V2 *>(pg + m * W);
+            const V2 ufl = *reinterpret_cast<const V2 *>(sUF + g * COLS + cl);
+            const V2 ufr = *reinterpret_cast<const V2 *>(sUF + N * COLS + g * COLS + cl);
+            const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
+            const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
+            const size_t obase = (size_t)Eg * sE_ + (size_t)g * sI + (size_t)Ag * sA + col;
+            T *pout = out + obase;
+            const T *prow = sIn + g * PS + P + wc;   // row slice F[g][j][element] at j = 0
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                const double uxd = a.u_nodes[Ag * N + j];
+                const double svd = accel * (nbfield * uxd);
+                const bool xpos = uxd >= 0.0;
+                const bool vpos = svd >= 0.0;
+                T dx0, dx1, dv0, dv1;
+                if constexpr (G::MMA) {
+                    // x: B rows m = t, 4 + t at column wc + g; lift rows xL (t = 0), xR (t = 1)
+                    const T *pb = sIn + j * W + P + wc + g;
+                    const T b0v = pb[t * PS];
+                    const T b1v = pb[(4 + t) * PS];
+                    const T *pxl = xpos ? (sXF + j * COLS + wc + g) : pb;
+                    const T *pxr = xpos ? (pb + (N - 1) * PS) : (sXF + N * COLS + j * COLS + wc + g);
+                    const T blv = (t < 2) ? *((t == 0) ? pxl : pxr) : (T)0;
+                    double x0 = 0.0, x1 = 0.0;
+                    dmma_8x8x4(x0, x1, ca0, b0v);
+                    dmma_8x8x4(x0, x1, ca1, b1v);
+                    dmma_8x8x4(x0, x1, calift, blv);
+                    // v: A = F[g][j][wc + 4c + t]; lift columns tL (t = 0), tR (t = 1)
+                    const T *pa = prow + j * W;
+                    const T a0v = pa[t];
+                    const T a1v = pa[4 + t];
+                    const int toff = (t == 0) ? (vpos ? -1 : 0) : (vpos ? N - 1 : N);
+                    const T alv = (t < 2) ? pa[toff] : (T)0;
+                    double v0 = 0.0, v1 = 0.0;
+                    dmma_8x8x4(v0, v1, a0v, ca0);
+                    dmma_8x8x4(v0, v1, a1v, ca1);
+                    dmma_8x8x4(v0, v1, alv, calift);
+                    dx0 = x0;
+                    dx1 = x1;
+                    dv0 = v0;
+                    dv1 = v1;
+                } else {
+                    const T *pc = sIn + j * W + P + cl;   // F[m][j][cl..cl+1] at m = 0
+                    dx0 = (T)0;
+                    dx1 = (T)0;
+                    V2 cm0, cm7;
+#pragma unroll
+                    for (int m = 0; m < N; ++m) {
+                        const V2 cv = *reinterpret_cast<const V2 *>(pc + m * PS);
+                        if (m == 0) cm0 = cv;
+                        if (m == N - 1) cm7 = cv;
+                        dx0 = fma(upi[m], cv.x, dx0);
+                        dx1 = fma(upi[m], cv.y, dx1);
+                    }
+                    const V2 xf0 = *reinterpret_cast<const V2 *>(sXF + j * COLS + cl);
+                    const V2 xf1 = *reinterpret_cast<const V2 *>(sXF + N * COLS + j * COLS + cl);
+                    const V2 xl = xpos ? xf0 : cm0;
+                    const V2 xr = xpos ? cm7 : xf1;
+                    dx0 = fma(xig0, xl.x, dx0);
+                    dx0 = fma(-xig1, xr.x, dx0);
+                    dx1 = fma(xig0, xl.y, dx1);
+                    dx1 = fma(-xig1, xr.y, dx1);
+                    const T *pa = prow + j * W;
+                    T line[N];
+                    load_line<N, (sizeof(T) == 8 ? 2 : 4), T>(pa, line);
+                    dv0 = (T)0;
+                    dv1 = (T)0;
+#pragma unroll
+                    for (int m = 0; m < N; ++m) {
+                        dv0 = fma(upk0[m], line[m], dv0);
+                        dv1 = fma(upk1[m], line[m], dv1);
+                    }
+                    const T tl = vpos ? pa[-1] : line[0];
+                    const T tr = vpos ? line[N - 1] : pa[N];
+                    dv0 = fma(xik00, tl, dv0);
+                    dv0 = fma(-xik01, tr, dv0);
+                    dv1 = fma(xik10, tl, dv1);
+                    dv1 = fma(-xik11, tr, dv1);
+                }
+                // u: sum_m up[j][m] F[g][m][k] + lifts (compile-time j: table constants)
+                T du0 = (T)0, du1 = (T)0;
+#pragma unroll
+                for (int m = 0; m < N; ++m) {
+                    du0 = fma(tb.up[j * N + m], fu[m].x, du0);
+                    du1 = fma(tb.up[j * N + m], fu[m].y, du1);
+                }
+                du0 = fma(tb.xi[2 * j], uL0, du0);
+                du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
+                du1 = fma(tb.xi[2 * j], uL1, du1);
+                du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
+                const T uxT = (T)uxd, svT = (T)svd;
+                const T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
+                const T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
+                const V2 fij = *reinterpret_cast<const V2 *>(prow + j * W + 2 * t);
+                V2 o;
+                if (kind == KIND_RHS) {
+                    o.x = r0;
+                    o.y = r1;
+                } else if (kind == KIND_EULER) {
+                    o.x = fma(dtT, r0, fij.x);
+                    o.y = fma(dtT, r1, fij.y);
+                } else {
+                    const V2 fnv = *reinterpret_cast<const V2 *>(sFn + g * PSF + j * WF + P + cl);
+                    o.x = fma(c2dt, r0, fma(c1, fij.x, c0 * fnv.x));
+                    o.y = fma(c2dt, r1, fma(c1, fij.y, c0 * fnv.y));
+                }
+                *reinterpret_cast<V2 *>(pout + j * sJ) = o;
+                if (gout != nullptr) {
+                    // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
+                    const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
+                    if (e == nx - 1) *reinterpret_cast<V2 *>(gout + gb) = fij;
+                    if (e == 0) *reinterpret_cast<V2 *>(gout + (size_t)(nx + 1) * sE_ + gb) = fij;
+                }
+                mk0 = fma(tb.wu[j], (double)o.x, mk0);
+                mk1 = fma(tb.wu[j], (double)o.y, mk1);
+            }
+        }
+        __syncthreads();   // stage s fully consumed
+        if (tid == 0 && q + 2 < ntile_cta) issue(s, q + 2);
+    }
+
+    if (a.partials == nullptr) return;
+    // moment partial of x node g: sum over the thread's columns, the quad, the warps
+    dd v = two_sum(tb.wv[2 * t] * mk0, tb.wv[2 * t + 1] * mk1);
+    v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 1), __shfl_xor_sync(0xffffffffu, v.lo, 1)});
+    v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 2), __shfl_xor_sync(0xffffffffu, v.lo, 2)});
+    if (t == 0) sRed[w][g] = v;
+    __syncthreads();
+    if (tid < N) {
+        dd s = sRed[0][tid];
+#pragma unroll
+        for (int ww = 1; ww < EPT; ++ww) s = dd_add(s, sRed[ww][tid]);
+        a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * N + tid] = s.hi + s.lo;
+    }
+    (void)NT;
+}
+
+}  // namespace vl
