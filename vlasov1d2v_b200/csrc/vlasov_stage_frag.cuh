@@ -30,6 +30,13 @@
 #include "vlasov_stage.cuh"
 #include "vlasov_stage_tma.cuh"
 
+#ifndef VL_FRAG_MINB64
+#define VL_FRAG_MINB64 2
+#endif
+#ifndef VL_FRAG_MINB32
+#define VL_FRAG_MINB32 4
+#endif
+
 namespace vl {
 
 template <typename T>
@@ -45,6 +52,7 @@ struct FragGeom {
     static constexpr int PSF = WF * ROWS;            // FN plane stride: 306 | 324
     static constexpr int THREADS = 32 * EPT;
     static constexpr bool MMA = sizeof(T) == 8;      // tensor-core x/v contractions (FP64)
+    static constexpr int MINB = sizeof(T) == 8 ? VL_FRAG_MINB64 : VL_FRAG_MINB32;   // CTAs per SM
     static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
     static constexpr size_t IN_B = al(sizeof(T) * (size_t)PS * N);
     static constexpr size_t FN_B = al(sizeof(T) * (size_t)PSF * N);
@@ -84,7 +92,7 @@ struct Pair<float> {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(FragGeom<T>::THREADS, 2)
+__global__ void __launch_bounds__(FragGeom<T>::THREADS, FragGeom<T>::MINB)
 stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                   const __grid_constant__ FragMaps maps) {
     using G = FragGeom<T>;
@@ -195,6 +203,13 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const int b0 = (tt - au * nbt) * EPT;
         const int nb = min(EPT, nv - b0);
         const int Ag = au + 1;
+        const bool act = w < nb;
+        const int col = (b0 + 1) * N + cl;   // global v-node column of the first output
+        // node coordinates of the tile, read before the wait so their latency overlaps it
+        double uxs[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) uxs[j] = a.u_nodes[Ag * N + j];
+        const double vn0 = act ? a.v_nodes[col] : 0.0, vn1 = act ? a.v_nodes[col + 1] : 0.0;
         if (!mbar_wait_bounded(&full[s], (uint32_t)((q >> 1) & 1))) {
             if (a.err != nullptr) atomicOr(a.err, 2);
             return;
@@ -204,10 +219,9 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
         const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
 
-        if (w < nb) {
-            const int col = (b0 + 1) * N + cl;   // global v-node column of the first output
-            const double sd0 = accel * (Ei + bfield * a.v_nodes[col]);
-            const double sd1 = accel * (Ei + bfield * a.v_nodes[col + 1]);
+        if (act) {
+            const double sd0 = accel * (Ei + bfield * vn0);
+            const double sd1 = accel * (Ei + bfield * vn1);
             const T sp0 = (T)sd0, sp1 = (T)sd1;
             // F[g][m][cl..cl+1] for the u contraction, and the u upwind traces
             const T *pg = sIn + g * PS + P + cl;
@@ -223,7 +237,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
             const T *prow = sIn + g * PS + P + wc;   // row slice F[g][j][element] at j = 0
 #pragma unroll
             for (int j = 0; j < N; ++j) {
-                const double uxd = a.u_nodes[Ag * N + j];
+                const double uxd = uxs[j];
                 const double svd = accel * (nbfield * uxd);
                 const bool xpos = uxd >= 0.0;
                 const bool vpos = svd >= 0.0;
