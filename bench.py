@@ -170,6 +170,23 @@ class Clocks:
 # ----------------------------------------------------------------------------------------------
 # GPU measurement
 # ----------------------------------------------------------------------------------------------
+def profiled_traffic_ratio(precision):
+    """DRAM bytes (read + write) per algorithmic byte of one fused stage launch, from the ncu
+    capture summarised in profiles/stage_frag_<precision>_16x50x50_n8.md (a half-size case of
+    the same kernel; the traffic scales with the elements processed).  None when absent."""
+    import re
+    path = os.path.join(ROOT, "profiles", f"stage_frag_{precision}_16x50x50_n8.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None, None
+    m = re.search(r"DRAM read / write \| ([0-9.]+) / ([0-9.]+) MB", text)
+    a = re.search(r"write s_\(i\+1\) = \d+ B/DOF = ([0-9.]+) MB", text)
+    if not m or not a:
+        return None, None
+    return (float(m.group(1)) + float(m.group(2))) / float(a.group(1)), os.path.relpath(path, ROOT)
+
+
 def measured_peak_hbm():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -368,12 +385,19 @@ def main():
         value = dist.sum(r["dof"] / (ms_step * 1e-3))
         stage_s = sum(r["stage_ms"]) * 1e-3
         achieved = sum(r["stage_bytes"]) / stage_s / 1e9
+        ratio, tsrc = profiled_traffic_ratio(prec)
+        per_launch = sum(r["stage_bytes"]) / len(r["stage_bytes"])
         e2e_s = dist.max(r["e2e_ms"]) * 1e-3
         out[prec] = {
             "value": value, "ms_per_step": ms_step,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": f"stage_kernel<{ORDER},{'double' if prec == 'fp64' else 'float'}>",
+                         "frac": achieved / peak,
+                         "traffic": None if ratio is None else ratio * per_launch,
+                         "traffic_note": None if ratio is None else
+                         f"bytes per launch (mean of the 3 stage kinds) = algorithmic x {ratio:.3f}, "
+                         f"the DRAM/algorithmic ratio of the ncu capture in {tsrc}",
+                         "algorithmic_bytes_per_launch": per_launch,
+                         "kernel": f"stage_frag_kernel<{'double' if prec == 'fp64' else 'float'}>",
                          "algorithmic_bytes_per_dof_step": r["bytes_per_dof_step"],
                          "stage_ms": r["stage_ms"], "field_ms": r["field_ms"],
                          "step_effective_gbs": r["dof"] * r["bytes_per_dof_step"] / (ms_step * 1e-3) / 1e9,
@@ -399,7 +423,8 @@ def main():
                    "buffers, 3 buffers)", "parallelism": f"replicas x{world}"},
         "roofline": head["roofline"],
         "e2e": head["e2e"],
-        "gpu_launches": 6 * args.steps + 1,
+        # per step: 3 fused stage kernels + 3 field solves of 2 kernels; one moment per call
+        "gpu_launches": 9 * args.steps + 1,
         "clocks": ck,
         "variants": {"fp32_mixed": {"value": out["fp32"]["value"], "dtype": "f32",
                                     "ms_per_step": out["fp32"]["ms_per_step"],
