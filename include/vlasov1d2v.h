@@ -183,6 +183,37 @@ VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, 
  * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */
 VL_API int vl_sync_ghosts(vl_ctx *ctx, void *f, void *stage, void *stream);
 
+/* ---- around the loop: initial state, post-processing ------------------------------------------
+ * These take the grid dimensions and state precision directly (no context): they need none of
+ * the context's tables.  prec is VL_FP64 or VL_FP32; arithmetic is FP64 in both. */
+
+/* Distribution.initialize_gpu (main/grid.py:244-279) and the eigenmode perturbation
+ * (main/grid.py:201-242), the O(DOF) part on the device:
+ *   f[e,i,a,j,b,k] = pol[a,j,b,k] * mx[e,i] + scale * (cx[e,i] vre[a,j,b,k] - sx[e,i] vim[a,j,b,k])
+ * pol = the loss-cone values factor * rsq^j exp(-rsq/2) on the velocity nodes incl. ghosts
+ * [(nu+2) n (nv+2) n]; mx = an x-node factor [(nx+2) n] or NULL (1); vre/vim = the eigenmode's
+ * velocity part (real, imaginary), cx/sx = cos/sin(k1 x) [(nx+2) n], scale = 2 delta_n; vre
+ * NULL = no perturbation.  The O(velocity) tables come from the host (Bessel series). */
+VL_API int vl_initial_state(void *f, int32_t prec, int32_t nx, int32_t nu, int32_t nv, int32_t n,
+                            const double *pol, const double *mx, const double *cx,
+                            const double *sx, const double *vre, const double *vim, double scale,
+                            void *stream);
+
+/* smooth_edges (main/grid.py:116-134): in place, the face-node planes of every interior element
+ * averaged with the neighbour's opposite face, x then u then v, left then right.  n >= 2. */
+VL_API int vl_smooth_edges(void *f, int32_t prec, int32_t nx, int32_t nu, int32_t nv, int32_t n,
+                           void *stream);
+
+/* Basis3D.interpolate_values (main/basis.py:291-317): values of the nodal polynomials on fine
+ * points of the elements lims = {x0, x1, u0, u1, v0, v1} (ghost-inclusive element indices,
+ * interior only, half-open).  ell_x[ex][n][fx] (ell_u, ell_v likewise) are the Lagrange
+ * polynomials at the fine points of each element of the range (host tables of the reference's
+ * construction); out[ex][fx][eu][fu][ev][fv] (FP64).  At most 32 fine points per element. */
+VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, int32_t nv,
+                          int32_t n, const int32_t *lims, const double *ell_x, const double *ell_u,
+                          const double *ell_v, int32_t fx, int32_t fu, int32_t fv, double *out,
+                          void *stream);
+
 /* ---- the loop without a caller-provided workspace ------------------------------------------- */
 
 /* No counterpart in the reference.  vl_ssp_rk3_steps for callers that cannot allocate device

@@ -456,3 +456,50 @@ def run(f, case: Case, final_time=None, steps=None, E0=None):
         dts.append(dt)
         energy.append(float(electric_energy(E, case)))
     return RunRecord(time_array=times, field_energy=energy, dt_history=dts, steps=count)
+
+
+# ---------------------------------------------------------------------------------------------
+# post-processing operators (main/grid.py:116-134, main/basis.py:291-317)
+# ---------------------------------------------------------------------------------------------
+def smooth_edges(arr):
+    """In place: each interior element's face-node planes averaged with the neighbour's
+    opposite face, x then u then v, left face then right face (``main/grid.py:116-134``); each
+    statement sees the previous ones, the right-hand side of each is evaluated first."""
+    r = np.roll
+    a = arr
+    a[1:-1, 0, 1:-1, :, 1:-1, :] = 0.5 * (r(a, 1, 0)[1:-1, -1, 1:-1, :, 1:-1, :] + a[1:-1, 0, 1:-1, :, 1:-1, :])
+    a[1:-1, -1, 1:-1, :, 1:-1, :] = 0.5 * (r(a, -1, 0)[1:-1, 0, 1:-1, :, 1:-1, :] + a[1:-1, -1, 1:-1, :, 1:-1, :])
+    a[1:-1, :, 1:-1, 0, 1:-1, :] = 0.5 * (r(a, 1, 2)[1:-1, :, 1:-1, -1, 1:-1, :] + a[1:-1, :, 1:-1, 0, 1:-1, :])
+    a[1:-1, :, 1:-1, -1, 1:-1, :] = 0.5 * (r(a, -1, 2)[1:-1, :, 1:-1, 0, 1:-1, :] + a[1:-1, :, 1:-1, -1, 1:-1, :])
+    a[1:-1, :, 1:-1, :, 1:-1, 0] = 0.5 * (r(a, 1, 4)[1:-1, :, 1:-1, :, 1:-1, -1] + a[1:-1, :, 1:-1, :, 1:-1, 0])
+    a[1:-1, :, 1:-1, :, 1:-1, -1] = 0.5 * (r(a, -1, 4)[1:-1, :, 1:-1, :, 1:-1, 0] + a[1:-1, :, 1:-1, :, 1:-1, -1])
+    return a
+
+
+def fine_points(axis: "Axis", num=25):
+    """25 equispaced points per element between its first and last node (``main/grid.py:38-42``)."""
+    return np.array([np.linspace(axis.arr[i, 0], axis.arr[i, -1], num=num)
+                     for i in range(1, axis.res + 1)])
+
+
+def fine_lagrange(basis: "Basis", axis: "Axis", lim, num=25):
+    """ell[e][i][p] = sum_s Vinv[s, i] P_s(xi_ep) for the elements lim[0] <= e < lim[1]
+    (ghost-inclusive indices) at their fine points (``main/basis.py:296-309``)."""
+    import scipy.special as sp
+
+    fine = fine_points(axis, num)                       # interior elements 1..res
+    mid = 0.5 * (axis.arr[1:-1, -1] + axis.arr[1:-1, 0])
+    xi = axis.J * (fine[lim[0] - 1:lim[1] - 1, :] - mid[lim[0] - 1:lim[1] - 1, None])
+    ps = np.array([sp.legendre(s)(xi) for s in range(basis.n)])
+    return np.transpose(np.tensordot(basis.vinv, ps, axes=([0], [0])), [1, 0, 2])
+
+
+def interpolate_values(arr, ell_x, ell_u, ell_v, limits):
+    """Tensor-product interpolation of the nodal state on the fine points of an element range
+    (``main/basis.py:310-317``): x, then u, then v contraction; out [ex, fx, eu, fu, ev, fv]."""
+    x_lim, u_lim, v_lim = limits
+    a = arr[x_lim[0]:x_lim[1], :, u_lim[0]:u_lim[1], :, v_lim[0]:v_lim[1], :]
+    val = np.multiply(ell_x[:, :, :, None, None, None, None], a[:, :, None, :, :, :, :]).sum(axis=1)
+    val = np.multiply(ell_u[None, None, :, :, :, None, None], val[:, :, :, :, None, :, :]).sum(axis=3)
+    val = np.multiply(ell_v[None, None, None, None, :, :, :], val[:, :, :, :, :, :, None]).sum(axis=5)
+    return val

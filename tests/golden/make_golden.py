@@ -187,8 +187,30 @@ def gen_cfg1(nsteps=200, out_name="cfg1_200", summary=True):
     np.savez_compressed(os.path.join(HERE, "cfg1_200.npz"), **out)
 
 
+def gen_post(res=(3, 3, 4), order=4, seed=5):
+    """Post-processing operators of the reference on a random state: smooth_edges
+    (main/grid.py:116-134) and Basis3D.interpolate_values (main/basis.py:291-317) on the
+    fine points of an element sub-range."""
+    refs = _refs()
+    orders = np.array([order] * 3)
+    basis = R.basis.Basis3D(orders)
+    L = 2.0 * np.pi / (0.886 / 10.0)
+    lows = np.array([-L / 2.0, -8.5 * refs.vt_e, -8.5 * refs.vt_e])
+    highs = np.array([L / 2.0, 8.5 * refs.vt_e, 8.5 * refs.vt_e])
+    grids = R.grid.Grid3D(basis=basis, lows=lows, highs=highs, resolutions=np.array(res),
+                          fine_all=True)
+    rng = np.random.default_rng(seed)
+    shape = (res[0] + 2, order, res[1] + 2, order, res[2] + 2, order)
+    state = rng.standard_normal(shape)
+    smoothed = _np(R.grid.smooth_edges(cp.asarray(state.copy())))
+    limits = np.array([[2, 3], [2, 3], [1, 3]])
+    interp = _np(basis.interpolate_values(grids, state, limits))
+    np.savez_compressed(os.path.join(HERE, "post.npz"), res=np.array(res), order=order,
+                        state=state, smoothed=smoothed, limits=limits, interp=interp)
+
+
 def main(argv):
-    which = argv or ["basis", "tiny", "small", "n8", "n9", "cfg1"]
+    which = argv or ["basis", "tiny", "small", "n8", "n9", "cfg1", "post"]
     if "basis" in which:
         gen_basis()
     if "tiny" in which:
@@ -201,6 +223,8 @@ def main(argv):
         gen_small("n9", (2, 2, 2), 9, 1, seed=4)
     if "cfg1" in which:
         gen_cfg1()
+    if "post" in which:
+        gen_post()
     if "cfg1_noise" in which:
         # the same run with a different BLAS thread count: the reference's own summation-order
         # noise floor for the energy history (run with OPENBLAS_NUM_THREADS=1)

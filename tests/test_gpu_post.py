@@ -1,0 +1,113 @@
+"""GPU parity of the kernels around the loop: initial-state construction on the device,
+smooth_edges and the fine-grid interpolation, against the reference's fixtures, the host
+construction (bit-identical to the reference's) and the CPU oracle."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import SMALL_CASES, case_setup, golden, rel_err
+from oracle import vlasov_oracle as vo
+
+pytestmark = pytest.mark.gpu
+
+
+def _grids(res, n, fine_all=False):
+    from vlasov1d2v_b200 import problem
+    from vlasov1d2v_b200.basis import Basis3D
+    from vlasov1d2v_b200.grid import Grid3D
+
+    refs = problem.default_reference()
+    basis = Basis3D(np.array([n] * 3))
+    L = 2.0 * np.pi / (0.886 / 10.0)
+    grids = Grid3D(basis, np.array([-L / 2, -8.5 * refs.vt_e, -8.5 * refs.vt_e]),
+                   np.array([L / 2, 8.5 * refs.vt_e, 8.5 * refs.vt_e]), np.array(res),
+                   fine_all=fine_all)
+    return refs, basis, grids
+
+
+@pytest.mark.parametrize("name", SMALL_CASES)
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_device_initial_state(cuda, name, precision):
+    """Eigenmode-perturbed loss cone built by vl_initial_state == the reference's f_init
+    (bit for bit in FP64; the FP32 state is its rounding)."""
+    from vlasov1d2v_b200.grid import Distribution
+
+    G, res, n = case_setup(name)
+    refs, basis, grids = _grids(res, n)
+    d = Distribution(vt=refs.vt_e, ring_j=6, resolutions=res, orders=[n] * 3, om=-0.349j,
+                     om_pc=10.0, delta_n=1.0e-3, perturbation=True, precision=precision)
+    d.initialize_gpu(grids)
+    f = d.arr.get()
+    if precision == "fp64":
+        np.testing.assert_array_equal(f, G["f_init"])
+    else:
+        np.testing.assert_array_equal(f, G["f_init"].astype(np.float32))
+
+
+def test_device_cos_initial_state(cuda):
+    """Benchmark initial state f0 (1 + a cos kx + noise) on the device == the host product."""
+    from vlasov1d2v_b200 import problem
+
+    p = problem.build((4, 6, 5), 8, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=3)
+    host = problem.cos_perturbed(p.grids, p.refs.vt_e, 6, 1.0e-3, noise=1.0e-6, seed=3)
+    np.testing.assert_array_equal(p.f.arr.get(), host)
+
+
+def test_smooth_edges_matches_reference(cuda):
+    from vlasov1d2v_b200.grid import smooth_edges
+
+    G = golden("post")
+    t = torch.as_tensor(G["state"].copy(), device="cuda")
+    out = smooth_edges(t)
+    np.testing.assert_array_equal(out.get(), G["smoothed"])
+    # the oracle restatement agrees with both
+    np.testing.assert_array_equal(vo.smooth_edges(G["state"].copy()), G["smoothed"])
+
+
+def test_smooth_edges_odd_shapes_against_oracle(cuda):
+    from vlasov1d2v_b200.grid import smooth_edges
+
+    rng = np.random.default_rng(11)
+    for shape in ((4, 3, 5, 3, 3, 3), (3, 5, 4, 5, 6, 5)):
+        a = rng.standard_normal(shape)
+        out = smooth_edges(torch.as_tensor(a.copy(), device="cuda")).get()
+        np.testing.assert_array_equal(out, vo.smooth_edges(a.copy()))
+
+
+def test_interpolate_values_matches_reference(cuda):
+    G = golden("post")
+    res, n = [int(r) for r in G["res"]], int(G["order"])
+    refs, basis, grids = _grids(res, n, fine_all=True)
+    lim = [tuple(int(v) for v in row) for row in G["limits"]]
+    out = basis.interpolate_values(grids, torch.as_tensor(G["state"], device="cuda"), lim).get()
+    assert out.shape == G["interp"].shape
+    assert rel_err(out, G["interp"]) <= 1e-14
+    host = basis.interpolate_values_host(grids, G["state"], lim)
+    assert rel_err(out, host) <= 1e-14
+
+
+def test_checkpoint_resume_is_exact(cuda, tmp_path):
+    """3 + 3 steps in one set of objects, or 3 + checkpoint + resume in fresh objects + 3:
+    identical (both make the same two loop calls, so the density summation order matches)."""
+    from vlasov1d2v_b200 import data_management as dm
+    from vlasov1d2v_b200 import problem
+
+    def fresh():
+        return problem.build((4, 6, 5), 4, perturbation="eigenmode", amp=1.0e-2)
+
+    a = fresh()
+    for _ in range(2):
+        a.stepper.run_steps(a.f, a.basis, a.elliptic, a.grids, a.flux, a.refs, 3)
+    b = fresh()
+    b.stepper.run_steps(b.f, b.basis, b.elliptic, b.grids, b.flux, b.refs, 3)
+    folder = str(tmp_path) + "/"
+    geo = np.array([[b.lows[d], b.highs[d], b.resolutions[d], b.orders[d]] for d in range(3)])
+    rd = dm.RunData(folder, "ck", b.f.shape, geo, np.array([1.0, 0.1, b.stepper.courant, 3]), b.refs)
+    rd.save_checkpoint(b.f, b.elliptic, b.stepper)
+    c = fresh()
+    c.stepper.resume_from(dm.ReadData(folder, "ck").read_checkpoint(), c.f, c.elliptic)
+    c.stepper.run_steps(c.f, c.basis, c.elliptic, c.grids, c.flux, c.refs, 3)
+    np.testing.assert_array_equal(c.f.arr.get(), a.f.arr.get())
+    np.testing.assert_array_equal(c.stepper.field_energy, a.stepper.field_energy)
+    np.testing.assert_array_equal(c.stepper.time_array, a.stepper.time_array)
+    assert c.stepper.steps_counter == a.stepper.steps_counter == 6

@@ -101,3 +101,15 @@ def test_cfg1_reference_noise_floor():
     a, b = golden("cfg1_200"), golden("cfg1_200_blas1")
     assert history_err(b["energy"], a["energy"]) < 1e-13
     np.testing.assert_allclose(b["time"], a["time"], rtol=1e-14)
+
+
+def test_post_processing_operators():
+    """smooth_edges and Basis3D.interpolate_values of the reference, pinned on a random state."""
+    G = golden("post")
+    res, n = [int(r) for r in G["res"]], int(G["order"])
+    assert np.array_equal(vo.smooth_edges(G["state"].copy()), G["smoothed"])
+    c = vo.make_case(*res, n)
+    lim = G["limits"]
+    ells = [vo.fine_lagrange(c.basis, ax, lim[d]) for d, ax in enumerate((c.x, c.u, c.v))]
+    out = vo.interpolate_values(G["state"], *ells, lim)
+    assert rel_err(out, G["interp"]) <= 1e-14

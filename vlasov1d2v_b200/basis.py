@@ -229,3 +229,54 @@ class Basis3D:
         self.b1 = Basis1D(orders[0])
         self.b2 = Basis1D(orders[1])
         self.b3 = Basis1D(orders[2])
+
+    @staticmethod
+    def _fine_lagrange(basis, grid, lim):
+        """ell[e][i][p]: the element's Lagrange polynomials at its fine points, for the elements
+        lim[0] <= e < lim[1] (ghost-inclusive indices), as ``main/basis.py:296-309`` builds
+        them (Legendre series through the inverse Vandermonde matrix).  Host FP64."""
+        xi = grid.J * (grid.arr_fine[lim[0]:lim[1], :] - grid.midpoints[lim[0] - 1:lim[1] - 1, None])
+        ps = np.array([sp.legendre(s)(xi) for s in range(basis.order)])
+        return np.ascontiguousarray(
+            np.transpose(np.tensordot(basis.vandermonde_inverse, ps, axes=([0], [0])), [1, 0, 2]))
+
+    def interpolate_values(self, grids, arr, limits):
+        """Values of the nodal state on the fine points of the elements in ``limits``
+        (``main/basis.py:291-317``): device kernel ``vl_interpolate``; returns a device array
+        [ex, fx, eu, fu, ev, fv] (FP64).  ``grids`` needs fine points in all three directions
+        (``Grid3D(..., fine_all=True)``)."""
+        import ctypes
+
+        import torch
+
+        from . import _device, _lib
+
+        t = _device.as_tensor(arr)
+        if t.dim() != 6:
+            raise ValueError("arr must be the 6-D state f[X, n, U, n, V, n]")
+        t = t.contiguous()
+        X, n, U, _, V, _ = t.shape
+        lims = [int(v) for pair in limits for v in pair]
+        ells = [self._fine_lagrange(b, g, lim) for b, g, lim in
+                ((self.b1, grids.x, limits[0]), (self.b2, grids.u, limits[1]), (self.b3, grids.v, limits[2]))]
+        dev = [torch.as_tensor(e, device=t.device) for e in ells]
+        fx, fu, fv = (e.shape[2] for e in ells)
+        ex, eu, ev = (lims[1] - lims[0], lims[3] - lims[2], lims[5] - lims[4])
+        out = torch.empty((ex, fx, eu, fu, ev, fv), dtype=torch.float64, device=t.device)
+        c_lims = (ctypes.c_int32 * 6)(*lims)
+        _lib.call("vl_interpolate", t.data_ptr(), _lib.VL_FP64 if t.dtype == torch.float64 else _lib.VL_FP32,
+                  X - 2, U - 2, V - 2, n, c_lims, dev[0].data_ptr(), dev[1].data_ptr(),
+                  dev[2].data_ptr(), fx, fu, fv, out.data_ptr(), _device.stream_handle())
+        return _device.wrap(out)
+
+    def interpolate_values_host(self, grids, arr, limits):
+        """Host NumPy form of ``interpolate_values`` (the reference's own expression)."""
+        ell_x, ell_u, ell_v = (self._fine_lagrange(b, g, lim) for b, g, lim in
+                               ((self.b1, grids.x, limits[0]), (self.b2, grids.u, limits[1]),
+                                (self.b3, grids.v, limits[2])))
+        x_lim, u_lim, v_lim = limits
+        arr_r = np.asarray(arr)[x_lim[0]:x_lim[1], :, u_lim[0]:u_lim[1], :, v_lim[0]:v_lim[1], :]
+        values = np.multiply(ell_x[:, :, :, None, None, None, None], arr_r[:, :, None, :, :, :, :]).sum(axis=1)
+        values = np.multiply(ell_u[None, None, :, :, :, None, None], values[:, :, :, :, None, :, :]).sum(axis=3)
+        values = np.multiply(ell_v[None, None, None, None, :, :, :], values[:, :, :, :, :, :, None]).sum(axis=5)
+        return values

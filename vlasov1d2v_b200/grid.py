@@ -124,17 +124,20 @@ class Grid3D:
 
 
 def smooth_edges(arr):
-    """Average each element-face node with its neighbour's (``main/grid.py:116-134``)."""
+    """Average each element-face node with its neighbour's (``main/grid.py:116-134``), in
+    place on the device (``vl_smooth_edges``: six passes in the reference's order).  Returns
+    the device array (a host array is copied to the device first)."""
     import torch
 
-    a = _device.as_tensor(arr)
-    a[1:-1, 0, 1:-1, :, 1:-1, :] = 0.5 * (torch.roll(a, 1, 0)[1:-1, -1, 1:-1, :, 1:-1, :] + a[1:-1, 0, 1:-1, :, 1:-1, :])
-    a[1:-1, -1, 1:-1, :, 1:-1, :] = 0.5 * (torch.roll(a, -1, 0)[1:-1, 0, 1:-1, :, 1:-1, :] + a[1:-1, -1, 1:-1, :, 1:-1, :])
-    a[1:-1, :, 1:-1, 0, 1:-1, :] = 0.5 * (torch.roll(a, 1, 2)[1:-1, :, 1:-1, -1, 1:-1, :] + a[1:-1, :, 1:-1, 0, 1:-1, :])
-    a[1:-1, :, 1:-1, -1, 1:-1, :] = 0.5 * (torch.roll(a, -1, 2)[1:-1, :, 1:-1, 0, 1:-1, :] + a[1:-1, :, 1:-1, -1, 1:-1, :])
-    a[1:-1, :, 1:-1, :, 1:-1, 0] = 0.5 * (torch.roll(a, 1, 4)[1:-1, :, 1:-1, :, 1:-1, -1] + a[1:-1, :, 1:-1, :, 1:-1, 0])
-    a[1:-1, :, 1:-1, :, 1:-1, -1] = 0.5 * (torch.roll(a, -1, 4)[1:-1, :, 1:-1, :, 1:-1, 0] + a[1:-1, :, 1:-1, :, 1:-1, -1])
-    return _device.wrap(a)
+    from . import _lib
+
+    t = _device.as_tensor(arr)
+    if t.dim() != 6 or not t.is_contiguous():
+        raise ValueError("arr must be a contiguous 6-D state f[X, n, U, n, V, n]")
+    X, n, U, _, V, _ = t.shape
+    _lib.call("vl_smooth_edges", t.data_ptr(), _lib.VL_FP64 if t.dtype == torch.float64 else _lib.VL_FP32,
+              X - 2, U - 2, V - 2, n, _device.stream_handle())
+    return _device.wrap(t)
 
 
 class Distribution:
@@ -237,9 +240,65 @@ class Distribution:
             arr = arr + self.eigenfunction(grids=grids)
         return arr
 
-    def initialize_gpu(self, grids):
+    def velocity_tables(self, grids):
+        """The O(velocity) parts of the initial state, host FP64: the loss-cone values
+        factor * rsq^j exp(-rsq/2) on the velocity nodes [U, n, V, n] (``main/grid.py:253-268``)
+        and, with a perturbation, the eigenmode's velocity part [U, n, V, n] (complex)."""
+        factor = 1.0 / ((2.0 ** self.ring_j) * (2.0 * np.pi) * (self.vt ** 2.0) *
+                        math.factorial(self.ring_j))
+        iu = np.tensordot(np.ones(grids.u.res_ghosts), np.ones(grids.u.order), axes=0)
+        iv = np.tensordot(np.ones(grids.v.res_ghosts), np.ones(grids.v.order), axes=0)
+        rsq = (np.tensordot(grids.u.arr ** 2.0, iv, axes=0) +
+               np.tensordot(iu, grids.v.arr ** 2.0, axes=0)) / (self.vt ** 2.0)
+        pol = factor * np.multiply(rsq ** self.ring_j, np.exp(-0.5 * rsq))
+        mode = None
+        if self.perturbation:
+            u = np.tensordot(grids.u.arr, np.ones_like(grids.v.arr), axes=0)
+            v = np.tensordot(np.ones_like(grids.u.arr), grids.v.arr, axes=0)
+            r = np.sqrt(u ** 2.0 + v ** 2.0)
+            phi = np.arctan2(v, u)
+            beta = - grids.x.k1 * r * self.om_pc
+            x = 0.5 * (r / self.vt) ** 2.0
+            f0 = 1 / (2.0 * np.pi * (self.vt ** 2.0) * math.factorial(self.ring_j)) * np.multiply(
+                x ** self.ring_j, np.exp(-x))
+            df_dv = np.multiply(f0, (self.ring_j / (x + 1.0e-16) - 1.0)) / (self.vt ** 2.0)
+            upsilon = np.array([n / (n - self.om) * np.multiply(sp.jv(n, beta), np.exp(-1j * n * phi))
+                                for n in range(-20, 21)]).sum(axis=0)
+            eig = np.multiply(df_dv, upsilon) / grids.x.k1 ** 2.0
+            mode = -1j * np.multiply(np.exp(1j * np.multiply(beta, np.sin(phi))), eig)
+        return pol, mode
+
+    def initialize_gpu(self, grids, x_factor=None):
+        """Build the initial state on the device (``vl_initial_state``): the O(DOF) tensor
+        product pol(u, v) [* x_factor(x)] [+ 2 delta_n Re(exp(i k1 x) mode(u, v))] is formed by
+        the kernel from the host's O(velocity) tables."""
+        import torch
+
+        from . import _lib
+
         self._grids = grids
-        self.set_array(self.initial_array(grids))
+        pol, mode = self.velocity_tables(grids)
+        dev = _device.device()
+        f = torch.empty(self.shape, dtype=self.dtype, device=dev)
+        keep = [torch.as_tensor(np.ascontiguousarray(pol), device=dev)]
+        ptr = lambda a: a.data_ptr() if a is not None else None
+        mx = None
+        if x_factor is not None:
+            mx = torch.as_tensor(np.ascontiguousarray(x_factor, dtype=np.float64), device=dev)
+        cx = sx = vre = vim = None
+        if mode is not None:
+            ph = np.exp(1j * grids.x.k1 * grids.x.arr)
+            cx = torch.as_tensor(np.ascontiguousarray(ph.real), device=dev)
+            sx = torch.as_tensor(np.ascontiguousarray(ph.imag), device=dev)
+            vre = torch.as_tensor(np.ascontiguousarray(mode.real), device=dev)
+            vim = torch.as_tensor(np.ascontiguousarray(mode.imag), device=dev)
+        _lib.call("vl_initial_state", f.data_ptr(),
+                  _lib.VL_FP64 if self.precision == "fp64" else _lib.VL_FP32,
+                  self.x_res, self.u_res, self.v_res, self.x_ord,
+                  keep[0].data_ptr(), ptr(mx), ptr(cx), ptr(sx), ptr(vre), ptr(vim),
+                  2.0 * self.delta_n, _device.stream_handle())
+        torch.cuda.current_stream().synchronize()   # the host tables are freed on return
+        self.arr = _device.wrap(f)
 
     def grid_order_gpu(self):
         self.arr = _device.wrap(self.arr.permute(0, 2, 4, 1, 3, 5).contiguous())

@@ -40,10 +40,10 @@ def loss_cone(grids, vt, ring_j):
     return d.initial_array(grids)
 
 
-def cos_perturbed(grids, vt, ring_j, amp, noise=0.0, seed=0):
-    """f0(u, v) (1 + amp cos(k1 x) + noise r(x)), k1 the fundamental mode of the x domain and
-    r uniform in [-1, 1] per interior x node (seeded; ghost x nodes take the periodic copy)."""
-    f0 = loss_cone(grids, vt, ring_j)
+def cos_x_factor(grids, amp, noise=0.0, seed=0):
+    """1 + amp cos(k1 x) + noise r(x) on the x nodes incl. ghosts, k1 the fundamental mode of
+    the x domain and r uniform in [-1, 1] per interior x node (seeded; ghost x nodes take the
+    periodic copy)."""
     k1 = 2.0 * np.pi / (grids.x.high - grids.x.low)
     mod = 1.0 + amp * np.cos(k1 * grids.x.arr)
     if noise:
@@ -54,7 +54,13 @@ def cos_perturbed(grids, vt, ring_j, amp, noise=0.0, seed=0):
         rr[0] = r[-1]
         rr[-1] = r[0]
         mod = mod + noise * rr
-    return f0 * mod[:, :, None, None, None, None]
+    return mod
+
+
+def cos_perturbed(grids, vt, ring_j, amp, noise=0.0, seed=0):
+    """Host FP64 f0(u, v) (1 + amp cos(k1 x) + noise r(x)) (see ``cos_x_factor``)."""
+    f0 = loss_cone(grids, vt, ring_j)
+    return f0 * cos_x_factor(grids, amp, noise, seed)[:, :, None, None, None, None]
 
 
 def build(res, order, *, om_pc=10.0, k=0.886, vmax=8.5, ring_j=6, perturbation="eigenmode",
@@ -80,8 +86,9 @@ def build(res, order, *, om_pc=10.0, k=0.886, vmax=8.5, ring_j=6, perturbation="
                         precision=precision)
     dist.initialize_quad_weights(grids)
     if perturbation == "cos":
-        dist.set_array(cos_perturbed(grids, refs.vt_e, ring_j, amp, noise=noise, seed=seed))
-        dist._grids = grids
+        # loss cone times the x factor, formed on the device (vl_initial_state)
+        dist.perturbation = False
+        dist.initialize_gpu(grids, x_factor=cos_x_factor(grids, amp, noise=noise, seed=seed))
     else:
         dist.initialize_gpu(grids)
     el = Elliptic(poisson_coefficient=refs.charge_density_multiplier)
@@ -104,4 +111,4 @@ def dof(res, order):
     return int(res[0] * res[1] * res[2]) * order ** 3
 
 
-__all__ = ["build", "cos_perturbed", "loss_cone", "default_reference", "dof"]
+__all__ = ["build", "cos_perturbed", "cos_x_factor", "loss_cone", "default_reference", "dof"]

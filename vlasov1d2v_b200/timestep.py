@@ -184,13 +184,32 @@ class Stepper:
         st.dt_hist = run.hist[2].data_ptr()
         return st
 
+    def resume_from(self, checkpoint, distribution, elliptic):
+        """Restore a checkpoint written by ``RunData.save_checkpoint`` (a dict as returned by
+        ``ReadData.read_checkpoint``): the state, the field and potential, the clock, dt, the
+        counters and the histories.  The next ``main_loop`` / ``run_steps`` continues the saved
+        run exactly (no initial energy entry, no dt re-adaptation)."""
+        distribution.set_array(checkpoint["f"])
+        elliptic.electric_field = _device.wrap(_device.as_tensor(checkpoint["E"]).clone())
+        elliptic.potential = _device.wrap(_device.as_tensor(checkpoint["phi"]).clone())
+        self.time = float(checkpoint["time"])
+        self.dt = float(checkpoint["dt"])
+        self.steps_counter = int(checkpoint["steps"])
+        self.write_counter = int(checkpoint["write_counter"])
+        self.time_array = np.array(checkpoint["time_array"], dtype=np.float64)
+        self.field_energy = np.array(checkpoint["field_energy"], dtype=np.float64)
+        self._resumed = True
+
     def main_loop(self, distribution, basis, elliptic, grids, dg_flux, refs, save_file):
         t0 = timer.time()
-        self.field_energy = np.append(self.field_energy, elliptic.electric_energy(grid=grids.x).get())
-        if self.verbose:
-            print('\nInitializing time-step...')
-        self.adapt_time_step(max_speeds=get_max_speeds(grids, elliptic, refs),
-                             dx=grids.x.dx, du=grids.u.dx, dv=grids.v.dx)
+        if getattr(self, "_resumed", False):
+            self._resumed = False
+        else:
+            self.field_energy = np.append(self.field_energy, elliptic.electric_energy(grid=grids.x).get())
+            if self.verbose:
+                print('\nInitializing time-step...')
+            self.adapt_time_step(max_speeds=get_max_speeds(grids, elliptic, refs),
+                                 dx=grids.x.dx, du=grids.u.dx, dv=grids.v.dx)
         run = self._run(distribution, elliptic, grids, refs)
         run.upload_state(self._host_state(run, self.final_time, _BIG_STEPS))
         batches = 0
@@ -237,7 +256,9 @@ class Stepper:
     def run_steps(self, distribution, basis, elliptic, grids, dg_flux, refs, nsteps):
         """Advance exactly ``nsteps`` steps (no final-time test) with the main loop's
         bookkeeping: energies and times appended, initial energy/dt from the current field."""
-        if self.dt is None or len(self.field_energy) == 0:
+        if getattr(self, "_resumed", False):
+            self._resumed = False
+        elif self.dt is None or len(self.field_energy) == 0:
             self.field_energy = np.append(self.field_energy,
                                           elliptic.electric_energy(grid=grids.x).get())
             self.adapt_time_step(max_speeds=get_max_speeds(grids, elliptic, refs),
