@@ -36,6 +36,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the batched-ensemble variant (64 heterogeneous FP32 members)")
+    ap.add_argument("--ensemble-steps", type=int, default=50)
     ap.add_argument("--kernel-reps", type=int, default=10)
     ap.add_argument("--kernel-only", action="store_true",
                     help="launch each stage kind --kernel-reps times on --res (profiling target)")
@@ -101,6 +104,54 @@ def cpu_port_rate(steps, warmup):
     t = (time.perf_counter() - t0) / max(steps, 1)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     return dof(SAMPLE_RES, ORDER) / t, t, cores
+
+
+def measure_ensemble(steps, warmup, members=64, seed=0):
+    """Batched heterogeneous ensemble (64 seeded FP32 members, orders 6-9, up to 2.4M DOF each):
+    aggregate DOF-updates/s of the ensemble driver (schedule from the autotuner), and of the same
+    members stepped one after another through the single-problem loop (each graph-captured)."""
+    import torch
+
+    from vlasov1d2v_b200.ensemble import Ensemble, build_members, sample_members
+
+    params = sample_members(members, seed=seed)
+    t0 = time.perf_counter()
+    probs = build_members(params, precision="fp32", seed=seed, batch_steps=max(steps, warmup))
+    ens = Ensemble(probs, batch_steps=max(steps, warmup))
+    setup_s = time.perf_counter() - t0
+    tune = ens.autotune(steps=3, use_cache=False, cache_path=None)
+    total = ens.total_dof()
+    ens.launch(warmup, use_graph=False)
+    ens.launch(steps, use_graph=True)   # capture
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    ens.launch(steps, use_graph=True)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    # the same members one after another, each through its own graph-captured loop
+    seq_ms = 0.0
+    for r in ens.runs:
+        r.launch(warmup, use_graph=False)
+        r.launch(steps, use_graph=True)
+        torch.cuda.synchronize()
+        c, d = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c.record()
+        r.launch(steps, use_graph=True)
+        d.record()
+        torch.cuda.synchronize()
+        seq_ms += c.elapsed_time(d) / steps
+        r.graph = None
+    orders = sorted({r.ctx.n for r in ens.runs})
+    return {"value": total / (ms * 1e-3), "unit": "DOF-updates/s", "dtype": "f32",
+            "ms_per_step": ms, "members": len(ens.runs), "total_dof": total, "orders": orders,
+            "schedule": tune["schedule"], "autotune_trials": len(tune["trials"]),
+            "sequential_single_runs_value": total / (seq_ms * 1e-3),
+            "speedup_vs_sequential": seq_ms / ms, "setup_s": setup_s,
+            "workload": "64 seeded loss-cone members: k~U[0.5,2], j in {3..6}, wp/wc~U[5,15], "
+                        "amp log-U[1e-4,1e-2], Nx in {8,16,32}, Nu=Nv in {24,32,40}, n in {6..9}, "
+                        "<= 2.4M DOF each"}
 
 
 def cpu_baseline_obj(steps=3, warmup=1):
@@ -431,6 +482,11 @@ def main():
                                     "roofline": out["fp32"]["roofline"], "e2e": out["fp32"]["e2e"],
                                     "speedup_vs_fp64": out["fp32"]["value"] / head["value"]}},
     }
+    if not args.no_ensemble:
+        try:
+            line["variants"]["ensemble_fp32"] = measure_ensemble(args.ensemble_steps, args.warmup)
+        except Exception as exc:  # the headline line must survive a failure of the extra
+            line["variants"]["ensemble_fp32"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline_obj()
     print(json.dumps(line))

@@ -178,6 +178,19 @@ VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, 
                      double *phi, vl_run_state *state, void *workspace, int nsteps,
                      void *stream);
 
+/* No counterpart in the reference (the FP32 mixed form).  Background split: the FP32 state
+ * holds delta f = f - f0(u, v), f0 an x-independent background kept in FP64 on the host side,
+ * so the x derivative no longer cancels the O(1) background against the O(1e-3) perturbation
+ * in FP32.  The stage kernels then add the RHS of f0 per node,
+ *   r0 = E_i eu + rb,
+ * with rb = J_u a B v D_u f0 + J_v (-a B u) D_v f0 and eu = J_u a D_u f0 precomputed in FP64
+ * and stored as float in the velocity-slab layout [(nu+2)][n][(nv+2)][n] (device pointers,
+ * 8-byte aligned, caller-owned, kept until the next call).  f0 is continuous across element
+ * faces, so its upwind and downwind face traces agree and one D_u table serves both signs of
+ * the u speed.  The x contraction of f0 is zero (f0 is constant in x).  Pass two NULLs to switch
+ * the split off.  FP32 contexts only.                                                         */
+VL_API int vl_set_background(vl_ctx *ctx, const float *rb, const float *eu);
+
 /* Copy f's ghost elements (all six ghost slabs) into a stage buffer and perform the
  * reference's periodic x-ghost swap on f (Distribution.swap_ghost_cells_of_array,
  * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */
@@ -213,6 +226,31 @@ VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, i
                           int32_t n, const int32_t *lims, const double *ell_x, const double *ell_u,
                           const double *ell_v, int32_t fx, int32_t fu, int32_t fv, double *out,
                           void *stream);
+
+/* ---- batched heterogeneous ensemble ------------------------------------------------------------
+ * No counterpart in the reference (which runs one problem per process).  Many independent
+ * problems -- each an ordinary context of any order 1..9 and grid, one common precision --
+ * advance together: per RK stage one forward-DFT launch, one inverse-DFT launch and one
+ * persistent stage kernel for all members, the stage kernel's CTAs walking a host-built list of
+ * (member, x element, tile group) work items balanced by estimated cost.  Members keep their own
+ * loop state (final time, histories); inactive members are skipped on the device.
+ *   vl_ens_create     members = existing contexts (borrowed; keep them alive)
+ *   vl_ens_bind       member i's state f, stage buffers, E, phi, loop state and workspace of
+ *                     vl_ens_workspace_bytes(ens, i) bytes (the stage buffers' velocity ghosts
+ *                     must equal f's, as for vl_ssp_rk3_steps)
+ *   vl_ens_schedule   tunables: threads per CTA (64 or 128), resident CTAs per SM, work items
+ *                     per CTA (tile groups per x slab follow from it)
+ *   vl_ens_commit     upload descriptors and the item list (synchronous; not inside a capture)
+ *   vl_ens_steps      nsteps SSP-RK3 steps of every member (stream-ordered, capturable)      */
+typedef struct vl_ens vl_ens;
+VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out);
+VL_API int vl_ens_destroy(vl_ens *ens);
+VL_API size_t vl_ens_workspace_bytes(const vl_ens *ens, int32_t i);
+VL_API int vl_ens_bind(vl_ens *ens, int32_t i, void *f, void *stage_a, void *stage_b, double *E,
+                       double *phi, vl_run_state *state, void *workspace);
+VL_API int vl_ens_schedule(vl_ens *ens, int32_t threads, int32_t ctas_per_sm, int32_t items_per_cta);
+VL_API int vl_ens_commit(vl_ens *ens);
+VL_API int vl_ens_steps(vl_ens *ens, int32_t nsteps, void *stream);
 
 /* ---- the loop without a caller-provided workspace ------------------------------------------- */
 

@@ -25,6 +25,8 @@ EXPORTED = (
     "vl_workspace_bytes", "vl_rhs", "vl_rhs_weighted", "vl_moment", "vl_poisson", "vl_field_energy", "vl_adapt_dt",
     "vl_rk_stage", "vl_run_state_init", "vl_ssp_rk3_steps", "vl_sync_ghosts",
     "vl_ssp_rk3_steps_noalloc", "vl_initial_state", "vl_smooth_edges", "vl_interpolate",
+    "vl_set_background", "vl_ens_create", "vl_ens_destroy", "vl_ens_workspace_bytes", "vl_ens_bind",
+    "vl_ens_schedule", "vl_ens_commit", "vl_ens_steps",
 )
 NOALLOC_SCRATCH_BYTES = 1 << 20
 
@@ -97,13 +99,23 @@ def _declare(lib):
     lib.vl_sync_ghosts.argtypes = [vp, vp, vp, vp]
     lib.vl_ssp_rk3_steps_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp]
     i32 = ctypes.c_int32
+    lib.vl_set_background.argtypes = [vp, vp, vp]
+    lib.vl_ens_create.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(vp)]
+    lib.vl_ens_destroy.argtypes = [vp]
+    lib.vl_ens_workspace_bytes.argtypes = [vp, i32]
+    lib.vl_ens_workspace_bytes.restype = ctypes.c_size_t
+    lib.vl_ens_bind.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp]
+    lib.vl_ens_schedule.argtypes = [vp, i32, i32, i32]
+    lib.vl_ens_commit.argtypes = [vp]
+    lib.vl_ens_steps.argtypes = [vp, i32, vp]
     lib.vl_initial_state.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp,
                                      ctypes.c_double, vp]
     lib.vl_smooth_edges.argtypes = [vp, i32, i32, i32, i32, i32, vp]
     lib.vl_interpolate.argtypes = [vp, i32, i32, i32, i32, i32, ctypes.POINTER(i32), vp, vp, vp,
                                    i32, i32, i32, vp, vp]
     for name in EXPORTED:
-        if name not in ("vl_last_error", "vl_abi_version", "vl_state_elems", "vl_workspace_bytes"):
+        if name not in ("vl_last_error", "vl_abi_version", "vl_state_elems", "vl_workspace_bytes",
+                        "vl_ens_workspace_bytes"):
             getattr(lib, name).restype = i
 
 

@@ -31,7 +31,7 @@ def run(res, order, steps, precision, perturbation="cos", amp=1.0e-3, noise=1.0e
     p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, steps)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
-    f = p.f.arr.as_subclass(torch.Tensor)
+    f = p.f.full_array().as_subclass(torch.Tensor)
     inner = f[1:-1, :, 1:-1, :, 1:-1, :].double().cpu().numpy()
     return {"time": np.asarray(p.stepper.time_array), "energy": np.asarray(p.stepper.field_energy),
             "f": inner, "wall_s": wall}

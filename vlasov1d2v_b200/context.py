@@ -167,6 +167,15 @@ class NativeContext:
         _lib.call("vl_rk_stage", self.handle, int(stage), _ptr(inp), _ptr(fn), _ptr(out), _ptr(E),
                   _ptr(dt), int(xhalo), _ptr(partials), ctypes.c_void_p(stream_handle()))
 
+    def set_background(self, tables):
+        """Install (tables = dict rb, eu of float32 device tensors) or clear (None) the
+        background-split RHS tables of the FP32 mixed form."""
+        self._bg = tables   # keep the tensors alive while the context refers to them
+        if tables is None:
+            _lib.call("vl_set_background", self.handle, None, None)
+        else:
+            _lib.call("vl_set_background", self.handle, _ptr(tables["rb"]), _ptr(tables["eu"]))
+
     def sync_ghosts(self, f, stage):
         self._check_state(f, "f")
         if stage is not None:

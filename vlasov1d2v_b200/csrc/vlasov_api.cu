@@ -22,30 +22,7 @@
 #include "vlasov_stage_tma.cuh"
 #include "vlasov_stage_frag.cuh"
 
-struct vl_ctx {
-    vl_config cfg;      // scalars (pointer members cleared)
-    int device;
-    int sm_count;
-    int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
-    int moment_grid_g;  // CTAs per x element of the standalone moment kernel
-    double up[vl::NMAX * vl::NMAX];
-    double xi[vl::NMAX * 2];
-    double xw[vl::NMAX];
-    double qw[vl::NMAX * vl::NMAX];
-    double *d_unodes = nullptr;
-    double *d_vnodes = nullptr;
-    double *d_k = nullptr;
-    double *d_xw = nullptr;
-    double2 *d_fwd = nullptr;
-    double2 *d_inv = nullptr;
-    double *d_tables = nullptr;   // up [n n], xi [n 2], qw [n n]
-    double *d_field = nullptr;    // field scratch of vl_poisson (mode coefficients)
-    double *d_moment = nullptr;   // moment partials of vl_moment [nx][moment_grid_g][n]
-    int *d_err = nullptr;         // device error word of operators run without a loop state
-    bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
-    bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
-    std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
-};
+#include "vlasov_ctx.cuh"
 
 namespace {
 
@@ -405,6 +382,8 @@ vl::StageArgs stage_args(const vl_ctx *c) {
     a.u_nodes = c->d_unodes;
     a.v_nodes = c->d_vnodes;
     a.tables = c->d_tables;
+    a.bg_rb = c->bg_rb;
+    a.bg_eu = c->bg_eu;
     a.nx = c->cfg.nx;
     a.nu = c->cfg.nu;
     a.nv = c->cfg.nv;
@@ -429,6 +408,10 @@ int upload(P **dst, const void *src, size_t bytes) {
 }  // namespace
 
 void vl_internal_set_error(const char *msg) { g_err = msg ? msg : ""; }
+
+int vl_internal_moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s) {
+    return moment(c, f, out, G, s);
+}
 
 extern "C" {
 
@@ -680,6 +663,18 @@ int vl_run_state_init(vl_ctx *c, vl_run_state *state, const double *E0, double f
     a.cap = cap;
     vl::scalars_kernel<<<1, vl::FIELD_THREADS, 0, as_stream(stream)>>>(a);
     return check_launch("scalars_kernel(init)");
+}
+
+int vl_set_background(vl_ctx *c, const float *rb, const float *eu) {
+    if (!c) return fail(VL_ERR_INVALID, "null context");
+    if ((rb == nullptr) != (eu == nullptr)) return fail(VL_ERR_INVALID, "background tables: give both or none");
+    if (rb && c->cfg.precision != VL_FP32)
+        return fail(VL_ERR_UNSUPPORTED, "the background split is a form of the FP32 context");
+    if ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(eu)) & 7)
+        return fail(VL_ERR_INVALID, "background tables must be 8-byte aligned");
+    c->bg_rb = rb;
+    c->bg_eu = eu;
+    return VL_OK;
 }
 
 int vl_sync_ghosts(vl_ctx *c, void *f, void *stage_buf, void *stream) {

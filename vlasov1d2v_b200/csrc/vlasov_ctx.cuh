@@ -1,0 +1,44 @@
+// Internal: the context object behind the opaque vl_ctx handle of the C ABI, shared by the
+// library's translation units (entry points, the ensemble driver).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <map>
+#include <utility>
+
+#include "vlasov1d2v.h"
+#include "vlasov_kernels.cuh"
+
+struct vl_ctx {
+    vl_config cfg;      // scalars (pointer members cleared)
+    int device;
+    int sm_count;
+    int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
+    int moment_grid_g;  // CTAs per x element of the standalone moment kernel
+    double up[vl::NMAX * vl::NMAX];
+    double xi[vl::NMAX * 2];
+    double xw[vl::NMAX];
+    double qw[vl::NMAX * vl::NMAX];
+    double *d_unodes = nullptr;
+    double *d_vnodes = nullptr;
+    double *d_k = nullptr;
+    double *d_xw = nullptr;
+    double2 *d_fwd = nullptr;
+    double2 *d_inv = nullptr;
+    double *d_tables = nullptr;   // up [n n], xi [n 2], qw [n n]
+    double *d_field = nullptr;    // field scratch of vl_poisson (mode coefficients)
+    double *d_moment = nullptr;   // moment partials of vl_moment [nx][moment_grid_g][n]
+    int *d_err = nullptr;         // device error word of operators run without a loop state
+    bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
+    bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
+    const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
+    const float *bg_eu = nullptr;
+    std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
+};
+
+
+// helpers of vlasov_api.cu used by the other translation units
+void vl_internal_set_error(const char *msg);
+int vl_internal_moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s);

@@ -1,0 +1,522 @@
+// Batched heterogeneous ensemble: many independent problems (different grids, orders and
+// physics) advanced by one set of launches per RK stage.
+//
+// Each member is an ordinary vl_ctx with its own state buffers and loop state.  Per RK stage the
+// ensemble issues three launches for all members together: the forward DFT of every member's
+// field solve, the inverse DFT (+ loop bookkeeping), and one persistent stage kernel whose CTAs
+// walk a precomputed list of work items (member, x element, tile group).  The item list is built
+// on the host by longest-processing-time-first assignment of estimated costs to CTAs, so members
+// of very different sizes share the device evenly.  The CTA count, block size and items per CTA
+// are the schedule's tunables (chosen by the autotuner in vlasov1d2v_b200/ensemble.py).
+//
+// The stage work of a member runs through the register-pencil tile body (orders 1..9) with
+// the order-specific up / xi tables in constant memory; the member's velocity weights and scalars
+// come from its descriptor.  Members whose loop state is inactive (final time reached) are
+// skipped by every kernel, so a batch of K steps is correct for members of any final time.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <queue>
+#include <string>
+#include <vector>
+
+#include "vlasov_ctx.cuh"
+#include "vlasov_stage.cuh"
+
+namespace vl {
+
+template <typename T>
+struct EnsTables {
+    T up[NMAX * NMAX];
+    T xi[NMAX * 2];
+};
+
+__constant__ EnsTables<double> c_ens64[NMAX + 1];
+__constant__ EnsTables<float> c_ens32[NMAX + 1];
+
+template <typename T>
+__device__ __forceinline__ const EnsTables<T> &ens_tables(int n);
+template <>
+__device__ __forceinline__ const EnsTables<double> &ens_tables<double>(int n) { return c_ens64[n]; }
+template <>
+__device__ __forceinline__ const EnsTables<float> &ens_tables<float>(int n) { return c_ens32[n]; }
+
+struct EnsMember {
+    StageArgs a;               // scalars and pointers; in / fn / out / kind set per stage
+    const void *f, *sa, *sb;   // the member's state and stage buffers
+    int n;
+    int G;                     // CTA groups per x element (moment partials per element)
+    double qw[NMAX * NMAX];    // w_j w_k / (J_u J_v)
+};
+
+struct EnsItem {
+    int member, e, g, pad;
+};
+
+// RK stage s of the nonlinear SSP-RK3 (main/timestep.py:157-163, :174-182)
+__device__ __forceinline__ void ens_stage_args(StageArgs &a, const EnsMember &m, int s) {
+    if (s == 0) {
+        a.in = m.f;
+        a.fn = nullptr;
+        a.out = const_cast<void *>(m.sa);
+        a.ghost_out = const_cast<void *>(m.f);
+        a.kind = KIND_EULER;
+    } else if (s == 1) {
+        a.in = m.sa;
+        a.fn = m.f;
+        a.out = const_cast<void *>(m.sb);
+        a.ghost_out = nullptr;
+        a.kind = KIND_COMBINE;
+        a.c0 = 3.0 / 4.0;
+        a.c1 = 1.0 / 4.0;
+        a.c2 = 1.0 / 4.0;
+    } else {
+        a.in = m.sb;
+        a.fn = m.f;
+        a.out = const_cast<void *>(m.f);
+        a.ghost_out = nullptr;
+        a.kind = KIND_COMBINE;
+        a.c0 = 1.0 / 3.0;
+        a.c1 = 2.0 / 3.0;
+        a.c2 = 2.0 / 3.0;
+    }
+}
+
+template <int N>
+struct EnsJC {
+    // j values per thread so that NT / 32 warps cover the n rows
+    template <int NT>
+    static constexpr int jc() { return (N + NT / 32 - 1) / (NT / 32); }
+};
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) ens_stage_kernel(const EnsMember *__restrict__ members,
+                                                      const int *__restrict__ cta_items,
+                                                      const EnsItem *__restrict__ items, int stage) {
+    __shared__ StageArgs sArgs;
+    __shared__ int sActive;
+    for (int it = cta_items[blockIdx.x]; it < cta_items[blockIdx.x + 1]; ++it) {
+        const EnsItem item = items[it];
+        const EnsMember &m = members[item.member];
+        __syncthreads();   // the previous item is done with the shared arguments and tiles
+        if (threadIdx.x == 0) {
+            StageArgs a = m.a;
+            ens_stage_args(a, m, stage);
+            sArgs = a;
+            sActive = (a.state == nullptr) || (a.state->active != 0);
+        }
+        __syncthreads();
+        if (!sActive) continue;
+        const int n = m.n;
+        switch (n) {
+#define VL_ENS_CASE(NN)                                                                            \
+    case NN:                                                                                       \
+        pencil_stage_body<NN, T, EnsJC<NN>::template jc<NT>(), NT, EnsTables<T>>(                 \
+            sArgs, ens_tables<T>(NN), m.qw,                                                        \
+                                                                     item.e, item.g, m.G);         \
+        break;
+            VL_ENS_CASE(1)
+            VL_ENS_CASE(2)
+            VL_ENS_CASE(3)
+            VL_ENS_CASE(4)
+            VL_ENS_CASE(5)
+            VL_ENS_CASE(6)
+            VL_ENS_CASE(7)
+            VL_ENS_CASE(8)
+            VL_ENS_CASE(9)
+#undef VL_ENS_CASE
+            default: break;
+        }
+    }
+}
+
+// field solves of all members: blockIdx.y = member, blockIdx.x = mode / node chunk
+__global__ void __launch_bounds__(FIELD_THREADS) ens_field_fwd_kernel(const FieldArgs *__restrict__ fa) {
+    const FieldArgs &a = fa[blockIdx.y];
+    if ((int)blockIdx.x * FWD_MODES >= a.M) return;
+    field_fwd_body(a, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(FIELD_THREADS) ens_field_inv_kernel(const FieldArgs *__restrict__ fa) {
+    const FieldArgs &a = fa[blockIdx.y];
+    const int nb = (a.nx * a.n + INV_NODES - 1) / INV_NODES;
+    if ((int)blockIdx.x >= nb) return;
+    field_inv_body(a, blockIdx.x, nb);
+}
+
+// clear every member's field ticket counter (start of a call)
+__global__ void ens_reset_kernel(const FieldArgs *__restrict__ fa, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) *reinterpret_cast<int *>(fa[i].scratch + 4 * (size_t)fa[i].M) = 0;
+}
+
+}  // namespace vl
+
+struct vl_ens {
+    std::vector<vl_ctx *> ctx;
+    int precision = VL_FP64;
+    int device = 0, sm_count = 148;
+    // binding per member
+    std::vector<vl::EnsMember> members;
+    std::vector<vl::FieldArgs> field[3];   // promote, require-active, record
+    std::vector<int> bound;
+    // schedule
+    int threads = 128, ctas = 0;
+    std::vector<int> G;
+    vl::EnsMember *d_members = nullptr;
+    vl::FieldArgs *d_field[3] = {nullptr, nullptr, nullptr};
+    int *d_cta_items = nullptr;
+    vl::EnsItem *d_items = nullptr;
+    int max_fwd = 1, max_inv = 1;
+    bool dirty = true;
+};
+
+namespace {
+
+int efail(int code, const std::string &msg) {
+    vl_internal_set_error(msg.c_str());
+    return code;
+}
+
+#define VL_ECUDA(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess) return efail(VL_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+int tiles_of(const vl_ctx *c) {
+    const int epw = 32 / c->cfg.n > 0 ? 32 / c->cfg.n : 1;
+    return c->cfg.nu * ((c->cfg.nv + epw - 1) / epw);
+}
+
+size_t partial_bytes(const vl_ctx *c, int G) {
+    const size_t b = sizeof(double) * (size_t)c->cfg.nx * G * c->cfg.n;
+    return (b + 255) & ~(size_t)255;
+}
+
+size_t field_bytes(const vl_ctx *c) {
+    const size_t b = sizeof(double) * vl::field_scratch_doubles(c->cfg.n_modes);
+    return (b + 255) & ~(size_t)255;
+}
+
+template <typename T>
+size_t ens_smem(int threads) {
+    size_t m = 0;
+    for (int n = 1; n <= vl::NMAX; ++n) {
+        const int rw = (32 / n) * n;
+        const size_t b = sizeof(double) * (size_t)n * threads + sizeof(T) * (size_t)(n * n * rw + n * n);
+        m = std::max(m, b);
+    }
+    return m;
+}
+
+template <typename T, int NT>
+int launch_stage(vl_ens *E, int stage, cudaStream_t s) {
+    const size_t smem = ens_smem<T>(NT);
+    vl::ens_stage_kernel<T, NT><<<E->ctas, NT, smem, s>>>(E->d_members, E->d_cta_items, E->d_items, stage);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_stage_kernel: ") + cudaGetErrorString(e));
+    return VL_OK;
+}
+
+int stage(vl_ens *E, int st, cudaStream_t s) {
+    if (E->precision == VL_FP64)
+        return E->threads == 64 ? launch_stage<double, 64>(E, st, s) : launch_stage<double, 128>(E, st, s);
+    return E->threads == 64 ? launch_stage<float, 64>(E, st, s) : launch_stage<float, 128>(E, st, s);
+}
+
+int field(vl_ens *E, int kind, cudaStream_t s) {
+    const int count = (int)E->ctx.size();
+    vl::ens_field_fwd_kernel<<<dim3(E->max_fwd, count), vl::FIELD_THREADS, 0, s>>>(E->d_field[kind]);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_fwd_kernel: ") + cudaGetErrorString(e));
+    vl::ens_field_inv_kernel<<<dim3(E->max_inv, count), vl::FIELD_THREADS, 0, s>>>(E->d_field[kind]);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_inv_kernel: ") + cudaGetErrorString(e));
+    return VL_OK;
+}
+
+template <typename T>
+int upload_tables(const std::vector<vl_ctx *> &ctxs) {
+    vl::EnsTables<T> tabs[vl::NMAX + 1];
+    std::memset(tabs, 0, sizeof(tabs));
+    for (const vl_ctx *c : ctxs) {
+        const int n = c->cfg.n;
+        for (int i = 0; i < n * n; ++i) tabs[n].up[i] = (T)c->up[i];
+        for (int i = 0; i < 2 * n; ++i) tabs[n].xi[i] = (T)c->xi[i];
+    }
+    if (sizeof(T) == 8)
+        VL_ECUDA(cudaMemcpyToSymbol(vl::c_ens64, tabs, sizeof(tabs)));
+    else
+        VL_ECUDA(cudaMemcpyToSymbol(vl::c_ens32, tabs, sizeof(tabs)));
+    return VL_OK;
+}
+
+// rebuild the device descriptors and the item list after a bind or schedule change
+int commit(vl_ens *E) {
+    const int count = (int)E->ctx.size();
+    for (int i = 0; i < count; ++i)
+        if (!E->bound[i]) return efail(VL_ERR_INVALID, "ensemble member " + std::to_string(i) + " is not bound");
+    // item costs: tiles per item x n^3 (DOFs per tile ~ 32 n^2, contraction length n)
+    struct Item {
+        double cost;
+        vl::EnsItem it;
+    };
+    std::vector<Item> items;
+    E->max_fwd = E->max_inv = 1;
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        const int G = E->G[i];
+        const double n = c->cfg.n;
+        const int tiles = tiles_of(c);
+        for (int e = 0; e < c->cfg.nx; ++e)
+            for (int g = 0; g < G; ++g) {
+                const int nt = (tiles - g + G - 1) / G;
+                items.push_back({nt * n * n * n, {i, e, g, 0}});
+            }
+        E->members[i].G = G;
+        for (int k = 0; k < 3; ++k) E->field[k][i].G = G;
+        E->max_fwd = std::max(E->max_fwd, (c->cfg.n_modes + vl::FWD_MODES - 1) / vl::FWD_MODES);
+        E->max_inv = std::max(E->max_inv, (c->cfg.nx * c->cfg.n + vl::INV_NODES - 1) / vl::INV_NODES);
+    }
+    // longest processing time first onto the least-loaded CTA
+    std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
+    const int P = std::max(1, std::min(E->ctas, (int)items.size()));
+    E->ctas = P;
+    std::vector<std::vector<vl::EnsItem>> per(P);
+    using Load = std::pair<double, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int p = 0; p < P; ++p) heap.push({0.0, p});
+    for (const Item &it : items) {
+        Load l = heap.top();
+        heap.pop();
+        per[l.second].push_back(it.it);
+        heap.push({l.first + it.cost, l.second});
+    }
+    std::vector<int> offs(P + 1, 0);
+    std::vector<vl::EnsItem> flat;
+    for (int p = 0; p < P; ++p) {
+        offs[p] = (int)flat.size();
+        flat.insert(flat.end(), per[p].begin(), per[p].end());
+    }
+    offs[P] = (int)flat.size();
+    cudaFree(E->d_cta_items);
+    cudaFree(E->d_items);
+    E->d_cta_items = nullptr;
+    E->d_items = nullptr;
+    VL_ECUDA(cudaMalloc((void **)&E->d_cta_items, sizeof(int) * offs.size()));
+    VL_ECUDA(cudaMalloc((void **)&E->d_items, sizeof(vl::EnsItem) * std::max<size_t>(flat.size(), 1)));
+    VL_ECUDA(cudaMemcpy(E->d_cta_items, offs.data(), sizeof(int) * offs.size(), cudaMemcpyHostToDevice));
+    VL_ECUDA(cudaMemcpy(E->d_items, flat.data(), sizeof(vl::EnsItem) * flat.size(), cudaMemcpyHostToDevice));
+    VL_ECUDA(cudaMemcpy(E->d_members, E->members.data(), sizeof(vl::EnsMember) * count, cudaMemcpyHostToDevice));
+    for (int k = 0; k < 3; ++k)
+        VL_ECUDA(cudaMemcpy(E->d_field[k], E->field[k].data(), sizeof(vl::FieldArgs) * count,
+                            cudaMemcpyHostToDevice));
+    E->dirty = false;
+    return VL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out) {
+    if (!ctxs || !out || count < 1) return efail(VL_ERR_INVALID, "need at least one context");
+    *out = nullptr;
+    vl_ens *E = new vl_ens();
+    E->precision = ctxs[0]->cfg.precision;
+    for (int i = 0; i < count; ++i) {
+        if (!ctxs[i]) {
+            delete E;
+            return efail(VL_ERR_INVALID, "null context");
+        }
+        if (ctxs[i]->cfg.precision != E->precision) {
+            delete E;
+            return efail(VL_ERR_INVALID, "ensemble members must share one precision");
+        }
+        if (ctxs[i]->cfg.n > 9) {
+            delete E;
+            return efail(VL_ERR_UNSUPPORTED, "ensemble members take orders 1..9");
+        }
+        if (ctxs[i]->bg_rb != nullptr) {
+            delete E;
+            return efail(VL_ERR_UNSUPPORTED, "ensemble members run without the background split");
+        }
+        E->ctx.push_back(ctxs[i]);
+    }
+    E->device = ctxs[0]->device;
+    E->sm_count = ctxs[0]->sm_count;
+    E->members.resize(count);
+    for (int k = 0; k < 3; ++k) E->field[k].resize(count);
+    E->bound.assign(count, 0);
+    E->G.assign(count, 1);
+    E->ctas = E->sm_count * 4;
+    std::memset(E->members.data(), 0, sizeof(vl::EnsMember) * count);
+    int rc = E->precision == VL_FP64 ? upload_tables<double>(E->ctx) : upload_tables<float>(E->ctx);
+    if (rc) {
+        delete E;
+        return rc;
+    }
+    cudaError_t e = cudaMalloc((void **)&E->d_members, sizeof(vl::EnsMember) * count);
+    for (int k = 0; k < 3 && e == cudaSuccess; ++k)
+        e = cudaMalloc((void **)&E->d_field[k], sizeof(vl::FieldArgs) * count);
+    if (e != cudaSuccess) {
+        vl_ens_destroy(E);
+        return efail(VL_ERR_CUDA, std::string("cudaMalloc(ensemble): ") + cudaGetErrorString(e));
+    }
+    for (int t : {64, 128}) {
+        const size_t smem = E->precision == VL_FP64 ? ens_smem<double>(t) : ens_smem<float>(t);
+        if (E->precision == VL_FP64)
+            cudaFuncSetAttribute(t == 64 ? vl::ens_stage_kernel<double, 64> : vl::ens_stage_kernel<double, 128>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        else
+            cudaFuncSetAttribute(t == 64 ? vl::ens_stage_kernel<float, 64> : vl::ens_stage_kernel<float, 128>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    }
+    *out = E;
+    return VL_OK;
+}
+
+VL_API int vl_ens_destroy(vl_ens *E) {
+    if (!E) return VL_OK;
+    cudaFree(E->d_members);
+    for (int k = 0; k < 3; ++k) cudaFree(E->d_field[k]);
+    cudaFree(E->d_cta_items);
+    cudaFree(E->d_items);
+    delete E;
+    return VL_OK;
+}
+
+VL_API size_t vl_ens_workspace_bytes(const vl_ens *E, int32_t i) {
+    if (!E || i < 0 || i >= (int)E->ctx.size()) return 0;
+    const vl_ctx *c = E->ctx[i];
+    return partial_bytes(c, tiles_of(c)) + field_bytes(c);   // partials for any schedule
+}
+
+VL_API int vl_ens_bind(vl_ens *E, int32_t i, void *f, void *sa, void *sb, double *Ef, double *phi,
+                       vl_run_state *state, void *workspace) {
+    if (!E || i < 0 || i >= (int)E->ctx.size()) return efail(VL_ERR_INVALID, "member index");
+    if (!f || !sa || !sb || !Ef || !state || !workspace) return efail(VL_ERR_INVALID, "null argument");
+    const vl_ctx *c = E->ctx[i];
+    vl::EnsMember &m = E->members[i];
+    std::memset(&m, 0, sizeof(m));
+    m.f = f;
+    m.sa = sa;
+    m.sb = sb;
+    m.n = c->cfg.n;
+    m.G = E->G[i];
+    std::memcpy(m.qw, c->qw, sizeof(m.qw));
+    vl::StageArgs &a = m.a;
+    a.E = Ef;
+    a.dt = &state->dt;
+    a.state = state;
+    a.err = &state->status;
+    a.u_nodes = c->d_unodes;
+    a.v_nodes = c->d_vnodes;
+    a.partials = static_cast<double *>(workspace);
+    a.tables = c->d_tables;
+    a.nx = c->cfg.nx;
+    a.nu = c->cfg.nu;
+    a.nv = c->cfg.nv;
+    a.xhalo = VL_XHALO_PERIODIC;
+    a.accel = c->cfg.accel;
+    a.bfield = c->cfg.bfield;
+    a.jx = c->cfg.jx;
+    a.ju = c->cfg.ju;
+    a.jv = c->cfg.jv;
+    double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) +
+                                                  partial_bytes(c, tiles_of(c)));
+    const int modes[3] = {vl::FIELD_PROMOTE, vl::FIELD_REQUIRE_ACTIVE,
+                          vl::FIELD_REQUIRE_ACTIVE | vl::FIELD_RECORD};
+    for (int k = 0; k < 3; ++k) {
+        vl::FieldArgs &fa = E->field[k][i];
+        std::memset(&fa, 0, sizeof(fa));
+        fa.partials = static_cast<double *>(workspace);
+        fa.G = m.G;
+        fa.E = Ef;
+        fa.phi = (k == 2) ? phi : nullptr;
+        fa.state = state;
+        fa.mode = modes[k];
+        fa.scratch = fscratch;
+        fa.fwd = c->d_fwd;
+        fa.inv = c->d_inv;
+        fa.k = c->d_k;
+        fa.xw = c->d_xw;
+        fa.nx = c->cfg.nx;
+        fa.n = c->cfg.n;
+        fa.M = c->cfg.n_modes;
+        fa.kappa = c->cfg.kappa;
+        fa.dx = c->cfg.dx;
+        fa.length = c->cfg.length_x;
+        fa.accel = c->cfg.accel;
+        fa.bfield = c->cfg.bfield;
+        fa.umax = c->cfg.umax;
+        fa.vmax = c->cfg.vmax;
+        fa.du = c->cfg.du;
+        fa.dv = c->cfg.dv;
+        fa.courant = c->cfg.courant;
+    }
+    E->bound[i] = 1;
+    E->dirty = true;
+    return VL_OK;
+}
+
+VL_API int vl_ens_schedule(vl_ens *E, int32_t threads, int32_t ctas_per_sm, int32_t items_per_cta) {
+    if (!E) return efail(VL_ERR_INVALID, "null ensemble");
+    if (threads != 64 && threads != 128) return efail(VL_ERR_INVALID, "threads must be 64 or 128");
+    if (ctas_per_sm < 1 || ctas_per_sm > 32 || items_per_cta < 1 || items_per_cta > 64)
+        return efail(VL_ERR_INVALID, "ctas_per_sm in 1..32, items_per_cta in 1..64");
+    E->threads = threads;
+    E->ctas = E->sm_count * ctas_per_sm;
+    // split each member's x slabs into tile groups so that the item count is about
+    // ctas x items_per_cta with items of similar cost
+    const int count = (int)E->ctx.size();
+    double total = 0.0;
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        const double n = c->cfg.n;
+        total += (double)c->cfg.nx * tiles_of(c) * n * n * n;
+    }
+    const double target = total / ((double)E->ctas * items_per_cta);
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        const double n = c->cfg.n;
+        const int tiles = tiles_of(c);
+        int G = (int)(tiles * n * n * n / target + 0.5);
+        E->G[i] = std::max(1, std::min(G, tiles));
+    }
+    E->dirty = true;
+    return VL_OK;
+}
+
+VL_API int vl_ens_commit(vl_ens *E) {
+    if (!E) return efail(VL_ERR_INVALID, "null ensemble");
+    return commit(E);
+}
+
+VL_API int vl_ens_steps(vl_ens *E, int32_t nsteps, void *stream) {
+    if (!E) return efail(VL_ERR_INVALID, "null ensemble");
+    if (nsteps < 0) return efail(VL_ERR_INVALID, "nsteps < 0");
+    if (E->dirty) return efail(VL_ERR_INVALID, "ensemble changed since the last vl_ens_commit");
+    int rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int count = (int)E->ctx.size();
+    vl::ens_reset_kernel<<<(count + 127) / 128, 128, 0, s>>>(E->d_field[0], count);
+    VL_ECUDA(cudaGetLastError());
+    // density partials of every member's f^n for the first field solve
+    for (int i = 0; i < count; ++i)
+        if ((rc = vl_internal_moment(E->ctx[i], E->members[i].f, E->members[i].a.partials, E->G[i], s)))
+            return rc;
+    for (int it = 0; it < nsteps; ++it) {
+        if ((rc = field(E, 0, s))) return rc;
+        if ((rc = stage(E, 0, s))) return rc;
+        if ((rc = field(E, 1, s))) return rc;
+        if ((rc = stage(E, 1, s))) return rc;
+        if ((rc = field(E, 2, s))) return rc;
+        if ((rc = stage(E, 2, s))) return rc;
+    }
+    return VL_OK;
+}
+
+}  // extern "C"

@@ -60,6 +60,12 @@ struct StageArgs {
     int kind;
     double c0, c1, c2;
     double accel, bfield, jx, ju, jv;
+    // Background split (FP32 mixed form): when bg_rb is not null the state holds the deviation
+    // from an x-independent background f0(u, v), and the RHS of f0 is added per node:
+    //   r0 = E_i * bg_eu + bg_rb,
+    // tables in the velocity-slab layout [U][n][V][n] (index a sA + j sJ + v column).
+    const float *bg_rb;
+    const float *bg_eu;
 };
 
 // ----------------------------------------------------------------------------------------------
@@ -172,7 +178,7 @@ __global__ void __launch_bounds__(MOMENT_THREADS, MOMENT_CTAS_PER_SM) moment_ker
 }
 
 // rho[e][i] = sum over g of the partials [e][g][i] (double-double, fixed order)
-__global__ void moment_reduce_kernel(const double *__restrict__ partials, double *__restrict__ rho,
+static __global__ void moment_reduce_kernel(const double *__restrict__ partials, double *__restrict__ rho,
                                      int nx, int G, int n) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nx * n) return;
@@ -255,13 +261,14 @@ __device__ __forceinline__ bool field_gate(const FieldArgs &a, bool first_cta) {
     return true;
 }
 
-__global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArgs a) {
+// CTA bx of the forward transform of one problem (modes 16 bx .. 16 bx + 15)
+__device__ __forceinline__ void field_fwd_body(const FieldArgs &a, int bx) {
     __shared__ double s_rhs[FIELD_MAX_NODES];
     __shared__ double s_cr[FIELD_PARTS][FWD_MODES + 1], s_ci[FIELD_PARTS][FWD_MODES + 1];
     __shared__ dd s_red[FIELD_THREADS / 32];
     static_assert(FIELD_PARTS * FWD_MODES == FIELD_THREADS && FIELD_PARTS == 64 &&
                       FWD_MODES <= FIELD_THREADS / 32, "forward thread layout");
-    if (!field_gate(a, blockIdx.x == 0)) return;
+    if (!field_gate(a, bx == 0)) return;
     const int tid = threadIdx.x;
     const int nn = a.nx * a.n;
     const int M = a.M;
@@ -289,7 +296,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArg
     }
     // this CTA's modes: thread (mode slot ml, part) sums nodes p = part, part + PARTS, ...
     const int ml = tid % FWD_MODES, part = tid / FWD_MODES;
-    const int m = blockIdx.x * FWD_MODES + ml;
+    const int m = bx * FWD_MODES + ml;
     double cr = 0.0, ci = 0.0;
     if (m < M) {
 #pragma unroll 4
@@ -305,7 +312,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArg
     __syncthreads();
     // warp w folds the 64 partial sums of mode slot w
     const int w = tid >> 5, lane = tid & 31;
-    const int mw = blockIdx.x * FWD_MODES + w;
+    const int mw = bx * FWD_MODES + w;
     if (w < FWD_MODES && mw < M) {
         double sr = s_cr[lane][w] + s_cr[lane + 32][w];
         double si = s_ci[lane][w] + s_ci[lane + 32][w];
@@ -336,7 +343,13 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArg
     }
 }
 
-__global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArgs a) {
+static __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArgs a) {
+    field_fwd_body(a, blockIdx.x);
+}
+
+// CTA bx of nblocks of the inverse transform of one problem (nodes 16 bx .. 16 bx + 15); the
+// last of the nblocks CTAs to finish does the loop bookkeeping
+__device__ __forceinline__ void field_inv_body(const FieldArgs &a, int bx, int nblocks) {
     __shared__ double2 s_E[FIELD_MAX_MODES];
     __shared__ double2 s_P[FIELD_MAX_MODES];
     __shared__ double s_er[FIELD_PARTS][INV_NODES + 1], s_pr[FIELD_PARTS][INV_NODES + 1];
@@ -357,7 +370,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArg
     }
     __syncthreads();
     const int nl = tid % INV_NODES, part = tid / INV_NODES;
-    const int p = blockIdx.x * INV_NODES + nl;
+    const int p = bx * INV_NODES + nl;
     double er = 0.0, pr = 0.0;
     if (p < nn) {
 #pragma unroll 4
@@ -376,7 +389,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArg
     __syncthreads();
     // warp w folds the 64 partial sums of node slot w
     const int w = tid >> 5, lane = tid & 31;
-    const int pw = blockIdx.x * INV_NODES + w;
+    const int pw = bx * INV_NODES + w;
     if (w < INV_NODES && pw < nn) {
         double se = s_er[lane][w] + s_er[lane + 32][w];
         double sp = s_pr[lane][w] + s_pr[lane + 32][w];
@@ -397,7 +410,7 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArg
     int *counter = reinterpret_cast<int *>(a.scratch + 4 * (size_t)M);
     __threadfence();
     __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(counter, 1) == (int)gridDim.x - 1);
+    if (tid == 0) s_last = (atomicAdd(counter, 1) == nblocks - 1);
     __syncthreads();
     if (!s_last) return;
     __threadfence();
@@ -441,6 +454,10 @@ __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArg
     }
 }
 
+static __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArgs a) {
+    field_inv_body(a, blockIdx.x, gridDim.x);
+}
+
 // energy + dt from a given E (vl_field_energy / vl_adapt_dt / vl_run_state_init)
 struct ScalarArgs {
     const double *E;
@@ -456,7 +473,7 @@ struct ScalarArgs {
     int cap;
 };
 
-__global__ void __launch_bounds__(FIELD_THREADS) scalars_kernel(const ScalarArgs a) {
+static __global__ void __launch_bounds__(FIELD_THREADS) scalars_kernel(const ScalarArgs a) {
     __shared__ dd s_red[FIELD_THREADS / 32];
     __shared__ double s_max[FIELD_THREADS / 32];
     const int nn = a.nx * a.n;

@@ -72,12 +72,16 @@ __device__ __forceinline__ void load_line(const T *p, T (&line)[N]) {
     }
 }
 
-template <int N, typename T>
-__global__ void __launch_bounds__(PencilGeom<N, T>::THREADS, PencilGeom<N, T>::MIN_BLOCKS)
-stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
-    using G = PencilGeom<N, T>;
-    constexpr int EPW = G::EPW, JC = G::JC, RW = G::RW, VEC = G::VEC, NT = G::THREADS;
-    if (a.state != nullptr && a.state->active == 0) return;
+// One CTA's share of a stage: x element e, tiles g, g + G, ... of that slab; writes the moment
+// partial [e][g][i] (of G per element).  JC_ j values per thread, NT_ threads per CTA: warps
+// beyond ceil(N / JC_) have no j chunk and only take part in the barriers and loads of shared
+// data (the ensemble kernel runs several orders with one block size).  tb supplies up / xi
+// (compile-time indices: parameter or constant bank); qw the velocity weights (w_j w_k/(J_u J_v)).
+template <int N, typename T, int JC_, int NT_, typename TB>
+__device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &tb, const double *qw,
+                                                  int e, int g, int G) {
+    using GP = PencilGeom<N, T>;
+    constexpr int EPW = GP::EPW, JC = JC_, RW = GP::RW, VEC = GP::VEC, NT = NT_;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sMom = reinterpret_cast<double *>(smem_raw);            // [N][THREADS]
     T *sF = reinterpret_cast<T *>(sMom + N * NT);                   // [N][N][RW]
@@ -87,10 +91,10 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int J0 = (tid >> 5) * JC;                 // warp-uniform j chunk
-    const int JN = min(JC, N - J0);
+    const int JN = min(JC, N - J0);                 // <= 0: a warp without a j chunk
     const int bl = lane / N, k = lane - (lane / N) * N;
     const bool lane_ok = lane < EPW * N;
-    if (tid < N) sE[tid] = a.E[(blockIdx.y + 1) * N + tid];
+    if (tid < N) sE[tid] = a.E[(e + 1) * N + tid];
 #pragma unroll
     for (int i = 0; i < N; ++i) sMom[i * NT + tid] = 0.0;
 
@@ -106,7 +110,6 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
     const int sI = sA * U;              // stride of i
     const size_t sE_ = (size_t)sI * N;  // stride of e
 
-    const int e = blockIdx.y;
     const int Eg = e + 1;
     int El, Er;
     if (a.xhalo == VL_XHALO_PERIODIC) {
@@ -130,12 +133,12 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
     const T xik0 = tb.xi[2 * kk], xik1 = tb.xi[2 * kk + 1];
     double wk[JC];
 #pragma unroll
-    for (int jc = 0; jc < JC; ++jc) wk[jc] = (jc < JN && lane_ok) ? tb.qw[(J0 + jc) * N + kk] : 0.0;
+    for (int jc = 0; jc < JC; ++jc) wk[jc] = (jc < JN && lane_ok) ? qw[(J0 + jc) * N + kk] : 0.0;
     __syncthreads();
 
     const int nbt = (nv + EPW - 1) / EPW;
     const int tiles = nu * nbt;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+    for (int t = g; t < tiles; t += G) {
         const int au = t / nbt;
         const int b0 = (t - au * nbt) * EPW;
         const int nb = min(EPW, nv - b0);
@@ -148,7 +151,7 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
 
         double ux[JC];
 #pragma unroll
-        for (int jc = 0; jc < JC; ++jc) ux[jc] = a.u_nodes[Ag * N + J0 + (jc < JN ? jc : 0)];
+        for (int jc = 0; jc < JC; ++jc) ux[jc] = a.u_nodes[Ag * N + (jc < JN ? J0 + jc : 0)];
         const double vnode = act ? a.v_nodes[col] : 0.0;
 
         // ---- own pencil columns (x lines) and the x upwind traces ----
@@ -275,7 +278,11 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
                 for (int m = 0; m < N; ++m) dv = fma(upk[m], line[m], dv);
                 dv = fma(xik0, vL, dv);
                 dv = fma(-xik1, vR, dv);
-                const T r = fma((T)ux[jc] * dx, jx, fma(s * du, ju, ((T)sv_d * dv) * jv));
+                T r = fma((T)ux[jc] * dx, jx, fma(s * du, ju, ((T)sv_d * dv) * jv));
+                if (a.bg_rb != nullptr) {   // RHS of the x-independent background
+                    const int vi = Ag * sA + j * sJ + col;
+                    r += (T)fmaf((float)sE[i], a.bg_eu[vi], a.bg_rb[vi]);
+                }
                 const T fij = rp[j * RW];
                 T o;
                 if (kind == KIND_RHS) {
@@ -320,8 +327,16 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
         for (int q = lane; q < NT; q += 32) v = dd_add(v, dd{sMom[i * NT + q], 0.0});
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) v = dd_add(v, shfl_down_dd(v, off));
-        if (lane == 0) a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * N + i] = v.hi + v.lo;
+        if (lane == 0) a.partials[((size_t)e * G + g) * N + i] = v.hi + v.lo;
     }
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(PencilGeom<N, T>::THREADS, PencilGeom<N, T>::MIN_BLOCKS)
+stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
+    if (a.state != nullptr && a.state->active == 0) return;
+    pencil_stage_body<N, T, PencilGeom<N, T>::JC, PencilGeom<N, T>::THREADS>(
+        a, tb, tb.qw, blockIdx.y, blockIdx.x, gridDim.x);
 }
 
 }  // namespace vl

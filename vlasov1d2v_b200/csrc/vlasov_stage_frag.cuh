@@ -318,8 +318,15 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                 du1 = fma(tb.xi[2 * j], uL1, du1);
                 du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
                 const T uxT = (T)uxd, svT = (T)svd;
-                const T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
-                const T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
+                T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
+                T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
+                if (a.bg_rb != nullptr) {   // RHS of the x-independent background
+                    const int vi = Ag * sA + j * sJ + col;
+                    const float2 eu = *reinterpret_cast<const float2 *>(a.bg_eu + vi);
+                    const float2 rb = *reinterpret_cast<const float2 *>(a.bg_rb + vi);
+                    r0 += (T)fmaf((float)Ei, eu.x, rb.x);
+                    r1 += (T)fmaf((float)Ei, eu.y, rb.y);
+                }
                 const V2 fij = *reinterpret_cast<const V2 *>(prow + j * W + 2 * t);
                 V2 o;
                 if (kind == KIND_RHS) {

@@ -322,7 +322,11 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                         dv = fma(xik0, line[0], dv);
                         dv = fma(-xik1, lp[N], dv);
                     }
-                    const T r = fma((T)ux[jc] * dx, jx, fma(sp * du, ju, ((T)sv_d * dv) * jv));
+                    T r = fma((T)ux[jc] * dx, jx, fma(sp * du, ju, ((T)sv_d * dv) * jv));
+                    if (a.bg_rb != nullptr) {   // RHS of the x-independent background
+                        const int vi = Ag * sA + j * sJ + col;
+                        r += (T)fmaf((float)sE[i], a.bg_eu[vi], a.bg_rb[vi]);
+                    }
                     const T fij = row[j];
                     T o;
                     if (kind == KIND_RHS) {

@@ -132,7 +132,8 @@ class RunData:
     def save_checkpoint(self, distribution, elliptic, stepper):
         """Full-precision restart point: state (ghosts included), field and potential, the
         stepper's time, dt, step and write counters and its histories."""
-        np.savez(self.checkpoint_name, f=_host(distribution.arr),
+        full = distribution.full_array() if hasattr(distribution, "full_array") else distribution.arr
+        np.savez(self.checkpoint_name, f=_host(full),
                  E=_host(elliptic.electric_field), phi=_host(elliptic.potential),
                  time=np.array(float(stepper.time)), dt=np.array(float(stepper.dt)),
                  steps=np.array(int(stepper.steps_counter)),

@@ -145,10 +145,16 @@ class Distribution:
 
     ``precision`` selects the state type: ``"fp64"`` (the reference's, default) or ``"fp32"``
     (mixed precision: FP32 state and contractions; FP64 moment, Poisson and energy).
+
+    ``background_split`` (FP32 only, default on): ``arr`` holds delta f = f - f0(u, v) with
+    f0 an x-independent FP64 background (the loss cone of the initial state, or the x-average of
+    a state given to ``set_array``).  The FP32 x derivative then acts on the O(perturbation)
+    part only instead of cancelling the O(1) background; the stage kernels add the FP64-built
+    RHS of f0.  ``full_array()`` returns f = f0 + delta f; ``moment_zero()`` the full density.
     """
 
     def __init__(self, vt, ring_j, resolutions, orders, perturbation=True, om=0.9, om_pc=1.0,
-                 delta_n=0.01, precision="fp64"):
+                 delta_n=0.01, precision="fp64", background_split=True):
         self.ring_j = ring_j
         self.vt = vt
         self.om = om
@@ -164,6 +170,9 @@ class Distribution:
         if precision not in ("fp64", "fp32"):
             raise ValueError("precision must be 'fp64' or 'fp32'")
         self.precision = precision
+        self.background_split = bool(background_split) and precision == "fp32"
+        self.background = None      # host FP64 f0[U, n, V, n] when split
+        self._bg_cache = {}
         self._grids = None
 
     @property
@@ -177,11 +186,78 @@ class Distribution:
         return (self.x_res + 2, self.x_ord, self.u_res + 2, self.u_ord, self.v_res + 2, self.v_ord)
 
     def set_array(self, arr):
-        """Install a host or device array as the state (cast to this distribution's precision)."""
+        """Install a host or device array as the state (cast to this distribution's precision).
+        With the background split, ``arr`` is the full f: its x-average (interior x nodes)
+        becomes the background f0 and the state holds f - f0."""
+        import torch
+
+        if self.background_split:
+            t = _device.as_tensor(arr, dtype=torch.float64)
+            if tuple(t.shape) != self.shape:
+                raise ValueError(f"state shape {tuple(t.shape)} != {self.shape}")
+            f0 = t[1:-1].mean(dim=(0, 1))
+            self._set_background(f0.cpu().numpy())
+            self.arr = _device.wrap((t - f0).to(self.dtype).contiguous())
+            return
         t = _device.as_tensor(arr, dtype=self.dtype)
         if tuple(t.shape) != self.shape:
             raise ValueError(f"state shape {tuple(t.shape)} != {self.shape}")
         self.arr = _device.wrap(t.contiguous())
+
+    def _set_background(self, f0):
+        self.background = np.ascontiguousarray(f0, dtype=np.float64)
+        self._bg_cache = {}
+
+    def full_array(self):
+        """The full state f (FP64 device array): f0 + delta f with the split, else ``arr``."""
+        import torch
+
+        t = _device.plain(self.arr)
+        if not self.background_split or self.background is None:
+            return _device.wrap(t)
+        f0 = torch.as_tensor(self.background, device=t.device)
+        return _device.wrap(t.double() + f0)
+
+    def background_tables(self, grids, accel, bfield):
+        """RHS tables of the background f0 for ``vl_set_background`` (host FP64 arithmetic,
+        stored float32 on the device), cached per (accel, B).  Velocity-slab layout
+        [U, n, V, n]; ghost entries zero.  f0 is continuous across element faces, so the u
+        derivative with the upwind lift of either side agrees (to rounding); the v direction's
+        upwind side depends on u only and is folded in."""
+        import torch
+
+        key = (float(accel), float(bfield))
+        if key in self._bg_cache:
+            return self._bg_cache[key]
+        f0 = self.background
+        n = self.u_ord
+        up = np.asarray(grids.u.basis.np_up, dtype=np.float64)
+        xi = np.asarray(grids.u.basis.np_xi, dtype=np.float64)
+        # u direction: contraction over j (axis 1) of f0[a, m, b, k]
+        cu = np.einsum("jm,ambk->ajbk", up, f0)
+        du = np.zeros_like(f0)
+        du[1:-1] = (cu[1:-1] + xi[None, :, 0, None, None] * f0[:-2, n - 1][:, None]
+                    - xi[None, :, 1, None, None] * f0[1:-1, n - 1][:, None])
+        # v direction: contraction over k (axis 3), upwind side from sv = -a B u
+        cv = np.einsum("km,ajbm->ajbk", up, f0)
+        sv = accel * (-bfield * grids.u.arr)                     # [U, n]
+        pos = (sv >= 0.0)[:, :, None, None]
+        left_p = xi[None, None, None, :, 0] * f0[:, :, :-2, n - 1][..., None] - xi[None, None, None, :, 1] * f0[:, :, 1:-1, n - 1][..., None]
+        left_m = xi[None, None, None, :, 0] * f0[:, :, 1:-1, 0][..., None] - xi[None, None, None, :, 1] * f0[:, :, 2:, 0][..., None]
+        dv = np.zeros_like(f0)
+        dv[:, :, 1:-1] = cv[:, :, 1:-1] + np.where(pos, left_p, left_m)
+        ju, jv = grids.u.J, grids.v.J
+        vv = grids.v.arr[None, None, :, :]                       # [1, 1, V, n]
+        rv = jv * sv[:, :, None, None] * dv
+        tabs = {"rb": ju * accel * bfield * vv * du + rv, "eu": ju * accel * du}
+        for t in tabs.values():   # only interior elements are read
+            t[0] = t[-1] = 0.0
+            t[:, :, 0] = t[:, :, -1] = 0.0
+        dev = _device.device()
+        out = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float32, device=dev)
+               for k, v in tabs.items()}
+        self._bg_cache[key] = out
+        return out
 
     def initialize_next(self):
         import torch
@@ -292,6 +368,12 @@ class Distribution:
             sx = torch.as_tensor(np.ascontiguousarray(ph.imag), device=dev)
             vre = torch.as_tensor(np.ascontiguousarray(mode.real), device=dev)
             vim = torch.as_tensor(np.ascontiguousarray(mode.imag), device=dev)
+        if self.background_split:
+            # the state is delta f = f - pol: the loss cone becomes the background
+            self._set_background(pol)
+            mx_host = (np.zeros(grids.x.arr.shape) if x_factor is None
+                       else np.asarray(x_factor, dtype=np.float64) - 1.0)
+            mx = torch.as_tensor(np.ascontiguousarray(mx_host), device=dev)
         _lib.call("vl_initial_state", f.data_ptr(),
                   _lib.VL_FP64 if self.precision == "fp64" else _lib.VL_FP32,
                   self.x_res, self.u_res, self.v_res, self.x_ord,
@@ -336,4 +418,10 @@ class Distribution:
         ctx = get_context(self._grids, precision=_device.precision_of(t))
         rho = torch.empty((self.x_res, self.x_ord), dtype=torch.float64, device=t.device)
         ctx.moment(t, rho)
+        if self.background_split and self.background is not None and t.data_ptr() == _device.plain(self.arr).data_ptr():
+            # + the density of the background (x-independent, FP64 on the host)
+            g = self._grids
+            qw = np.tensordot(g.u.np_quad_weights, g.v.np_quad_weights, axes=0) / (g.u.J * g.v.J)
+            rho0 = float(np.sum(self.background[1:-1, :, 1:-1, :] * qw))
+            rho = rho + rho0
         return _device.wrap(rho)

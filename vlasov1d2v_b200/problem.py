@@ -65,7 +65,7 @@ def cos_perturbed(grids, vt, ring_j, amp, noise=0.0, seed=0):
 
 def build(res, order, *, om_pc=10.0, k=0.886, vmax=8.5, ring_j=6, perturbation="eigenmode",
           amp=1.0e-3, noise=0.0, seed=0, precision="fp64", final_time=2.0, write_time=0.1,
-          om=-0.349j, batch_steps=32, verbose=False):
+          om=-0.349j, batch_steps=32, verbose=False, background_split=True):
     """Build (refs, basis, grids, distribution, elliptic, flux, stepper) on the current device.
 
     ``perturbation``: ``"eigenmode"`` (the reference's Bessel-series mode with amplitude
@@ -83,7 +83,7 @@ def build(res, order, *, om_pc=10.0, k=0.886, vmax=8.5, ring_j=6, perturbation="
     grids = Grid3D(basis=basis, lows=lows, highs=highs, resolutions=resolutions)
     dist = Distribution(vt=refs.vt_e, ring_j=ring_j, resolutions=resolutions, orders=orders,
                         om=om, om_pc=om_pc, delta_n=amp, perturbation=(perturbation == "eigenmode"),
-                        precision=precision)
+                        precision=precision, background_split=background_split)
     dist.initialize_quad_weights(grids)
     if perturbation == "cos":
         # loss cone times the x factor, formed on the device (vl_initial_state)

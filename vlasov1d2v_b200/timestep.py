@@ -75,6 +75,7 @@ class _Run:
         self.graph = None
         self.graph_steps = 0
         self.synced_ptr = None
+        self.background = None   # RHS tables of the FP32 background split, or None
 
     def upload_state(self, st: _lib.VlRunState):
         host = torch.frombuffer(bytearray(bytes(st)), dtype=torch.uint8)
@@ -90,6 +91,15 @@ class _Run:
         self.synced_ptr = self.f.data_ptr()
 
     def launch(self, nsteps, use_graph):
+        # the background tables ride in the stage kernels' launch parameters: install them on
+        # the (shared) context for these launches only
+        self.ctx.set_background(self.background)
+        try:
+            self._launch(nsteps, use_graph)
+        finally:
+            self.ctx.set_background(None)
+
+    def _launch(self, nsteps, use_graph):
         if not use_graph:
             self.ctx.ssp_rk3_steps(self.f, self.sa, self.sb, self.E, self.phi, self.state, nsteps)
             return
@@ -162,6 +172,11 @@ class Stepper:
         if run is None:
             run = _Run(ctx, f, hist_cap=max(self.batch_steps, 1))
             self._runs = {key: run}
+        if getattr(distribution, "background_split", False) and distribution.background is not None:
+            run.background = distribution.background_tables(
+                grids, refs.electron_acceleration_multiplier, elliptic.magnetic_field)
+        else:
+            run.background = None
         # stage buffers take f's ghost elements (the inflow boundary values) and f gets the
         # periodic x-ghost swap, as main/timestep.py:143-151 does at every step
         run.sync_ghosts()
