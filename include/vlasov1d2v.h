@@ -252,6 +252,47 @@ VL_API int vl_ens_schedule(vl_ens *ens, int32_t threads, int32_t ctas_per_sm, in
 VL_API int vl_ens_commit(vl_ens *ens);
 VL_API int vl_ens_steps(vl_ens *ens, int32_t nsteps, void *stream);
 
+/* ---- learned coarse-grid closure ------------------------------------------------------------------
+ * No counterpart in the reference.  A per-(x node, velocity element) MLP corrects the RHS of a
+ * coarse (order 6) velocity grid towards the L2 projection of a fine-grid RHS.
+ * Network: IN = 96 inputs -> 128 -> 128 -> 128 (GELU) -> OUT = 48 outputs (first 36 used),
+ * bf16 weights and activations, FP32 accumulation (tensor cores, mma m16n8k16).  Weights live
+ * in two bf16 layouts, wf = [out][in] and wb = [in][out] per layer, layers back to back
+ * (layer offsets 0, 96*128, 96*128 + 128*128, 96*128 + 2*128*128; n_weights elements), and
+ * FP32 biases (offsets 0, 128, 256, 384; n_bias elements); vl_mlp_dims reports the sizes.    */
+VL_API int vl_mlp_dims(int32_t *in, int32_t *hidden, int32_t *out, int32_t *n_weights, int32_t *n_bias);
+/* Y[nrows][48] = MLP(X[nrows][96]).  With H0 [nrows][96] bf16, Hh [3][nrows][128] bf16 and
+ * Z [3][nrows][128] FP32 given, the layer inputs and hidden pre-activations are kept for
+ * vl_mlp_backward (all three or none).                                                      */
+VL_API int vl_mlp_forward(const float *X, int32_t nrows, const void *wf, const void *wb, const float *bias,
+                          float *Y, void *H0, void *Hh, float *Z, void *stream);
+/* FP32 elements of the per-block gradient partials vl_mlp_backward needs for nrows samples. */
+VL_API size_t vl_mlp_partial_floats(int32_t nrows);
+/* Gradient of L = sum_{rows, c < nout} (Y - T)^2 / (nrows nout), T[nrows][nout], through the
+ * network (bf16 operands, FP32 accumulation; per-block partials summed in a fixed order):
+ * grad_w in the [in][out] layout, grad_b.                                                    */
+VL_API int vl_mlp_backward(const float *Y, const float *T, int32_t nrows, int32_t nout, const void *wf,
+                           const void *wb, const float *bias, const void *H0, const void *Hh, const float *Z,
+                           float *partials, float *grad_w, float *grad_b, void *stream);
+/* One Adam step (step >= 1: bias corrections) on FP32 master weights ([in][out]) and biases,
+ * with decoupled weight decay; refreshes both bf16 layouts.                                   */
+VL_API int vl_mlp_adam(float *master_w, float *master_b, const float *grad_w, const float *grad_b, float *m_w,
+                       float *v_w, float *m_b, float *v_b, void *wf, void *wb, float lr, float beta1,
+                       float beta2, float eps, int32_t step, float weight_decay, void *stream);
+/* Closure inputs of a coarse state f (order 6): one sample per (x node, interior velocity
+ * element), X[nx*6*nu*nv][96] (84 state values divided by the sample's scale max|.|, then
+ * a E_i / escale, u / umax and v / vmax of the element centre, a B, zeros), scale[samples].  */
+VL_API int vl_closure_features(const void *f, int32_t prec, int32_t nx, int32_t nu, int32_t nv,
+                               const double *E, double accel, double bfield, const double *u_nodes,
+                               const double *v_nodes, double umax, double vmax, double escale, float *X,
+                               float *scale, void *stream);
+/* out[e, i, a, j, b, k] += c2 * (*dt) * cscale * scale[s] * clamp(Y[s][6 j + k], +-ymax) for
+ * every interior node: the network's RHS correction applied to an RK stage output, its outputs
+ * clamped to the range seen in training (state may be NULL; an inactive loop state skips it).  */
+VL_API int vl_closure_apply(void *out, int32_t prec, int32_t nx, int32_t nu, int32_t nv, const float *Y,
+                            const float *scale, double cscale, float ymax, const double *dt, double c2,
+                            const vl_run_state *state, void *stream);
+
 /* ---- the loop without a caller-provided workspace ------------------------------------------- */
 
 /* No counterpart in the reference.  vl_ssp_rk3_steps for callers that cannot allocate device

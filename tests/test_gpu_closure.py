@@ -1,0 +1,116 @@
+"""The learned closure on the GPU: the network's forward and backward kernels against the CPU
+oracle, training, the closure loop's plain (fallback) form against the standard coarse loop, and
+what the trained network gains over the coarse RHS without it."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import history_err, rel_err
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+def _weights(mlp):
+    W = [w.float().cpu().numpy().astype(np.float64) for w in mlp.layer_views(mlp.wb)]
+    b, off = [], 0
+    for (_, n) in mlp.LAYERS:
+        b.append(mlp.master_b[off:off + n].cpu().numpy().astype(np.float64))
+        off += n
+    return W, b
+
+
+def test_mlp_gradients_against_oracle(cuda):
+    from vlasov1d2v_b200.closure import MLP
+
+    mlp = MLP(seed=1)
+    rng = np.random.default_rng(3)
+    n, nout = 200, 36
+    X = rng.normal(size=(n, mo.IN)).astype(np.float32)
+    X[:, 88:] = 0.0
+    T = rng.normal(size=(n, nout)).astype(np.float32)
+    Xd, Td = torch.as_tensor(X, device="cuda"), torch.as_tensor(T, device="cuda")
+    buf = mlp.buffers(n, Xd.device)
+    Y = mlp.gradients(Xd, Td, buf).cpu().numpy().astype(np.float64)
+    W, b = _weights(mlp)
+    Yo, H, Z = mo.forward(X, W, b)
+    assert rel_err(Y, Yo) < 2e-3
+    # backward from the GPU's outputs so that both start from the same loss gradient
+    dW, db = mo.backward(Y, T.astype(np.float64), W, H, Z, nout)
+    gw = mlp.layer_views(mlp.grad_w)
+    off = 0
+    gb = []
+    for (_, m) in mlp.LAYERS:
+        gb.append(mlp.grad_b[off:off + m].cpu().numpy())
+        off += m
+    for l in range(4):
+        g = gw[l].cpu().numpy()
+        err = np.linalg.norm(g - dW[l]) / np.linalg.norm(dW[l])
+        errb = np.linalg.norm(gb[l] - db[l]) / np.linalg.norm(db[l])
+        print(f"layer {l}: dW normwise {err:.2e}, db {errb:.2e}")
+        assert err < 1e-2 and errb < 1e-2
+
+
+def test_training_fits_a_smooth_map(cuda):
+    from vlasov1d2v_b200.closure import MLP, evaluate, train
+
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    n = 16384
+    X = torch.randn((n, mo.IN), device="cuda", generator=g)
+    X[:, 88:] = 0.0
+    A = torch.randn((mo.IN, 36), device="cuda", generator=g) / 10.0
+    T = torch.tanh(X @ A).contiguous()
+    mlp = MLP(seed=2)
+    before = evaluate(mlp, X, T)
+    hist = train(mlp, X, T, epochs=20, batch=2048, lr=3e-3)
+    after = evaluate(mlp, X, T)
+    assert after < before / 4, (before, after, hist[-1])
+
+
+def _coarse(res=(4, 5, 5), amp=0.02):
+    from vlasov1d2v_b200 import problem
+
+    return problem.build(res, 6, perturbation="cos", amp=amp, batch_steps=4)
+
+
+def test_closure_loop_fallback_matches_plain_coarse(cuda):
+    """With no network the closure loop is the plain coarse solver (its fallback)."""
+    from vlasov1d2v_b200.closure import ClosureStepper
+
+    a = _coarse()
+    a.stepper.run_steps(a.f, a.basis, a.elliptic, a.grids, a.flux, a.refs, 8)
+    b = _coarse()
+    cs = ClosureStepper(b, mlp=None)
+    cs.run_steps(8, batch=4)
+    assert rel_err(b.f.arr.get(), a.f.arr.get()) < 1e-12
+    assert history_err(cs.energies, a.stepper.field_energy) < 1e-12
+    np.testing.assert_allclose(cs.times, a.stepper.time_array, rtol=1e-13)
+
+
+def test_trained_closure_gains_over_plain_coarse_rhs(cuda):
+    """Fine runs (order 8, 3x the velocity elements) projected to the coarse grid: the trained
+    network's correction brings the coarse RHS closer to the projected fine RHS on held-out
+    snapshots than the coarse RHS alone."""
+    from vlasov1d2v_b200 import problem
+    from vlasov1d2v_b200.basis import Basis1D
+    from vlasov1d2v_b200.closure import MLP, Projector, evaluate, make_pair, train
+
+    proj = Projector(np.asarray(Basis1D(8).nodes, float), np.asarray(Basis1D(6).nodes, float), 3)
+    Xs, Ts = [], []
+    for draw, (k, ompc) in enumerate([(0.886, 10.0), (1.2, 8.0), (0.7, 12.0)]):
+        fine = problem.build((4, 12, 12), 8, k=k, om_pc=ompc, perturbation="cos", amp=0.05, batch_steps=10)
+        coarse = problem.build((4, 4, 4), 6, k=k, om_pc=ompc, perturbation="cos", amp=0.05)
+        for snap in range(4):
+            fine.stepper.run_steps(fine.f, fine.basis, fine.elliptic, fine.grids, fine.flux, fine.refs, 10)
+            X, T = make_pair(fine, coarse, proj, escale=1.0)
+            Xs.append(X)
+            Ts.append(T)
+    Xtr, Ttr = torch.cat(Xs[:-2]), torch.cat(Ts[:-2])
+    Xva, Tva = torch.cat(Xs[-2:]), torch.cat(Ts[-2:])
+    mlp = MLP(seed=0)
+    zero = float((Tva ** 2).mean())   # error of the coarse RHS without correction
+    train(mlp, Xtr, Ttr, epochs=40, batch=256, lr=2e-3)
+    after = evaluate(mlp, Xva, Tva)
+    print(f"held-out RHS error: plain coarse {zero:.3e}, with closure {after:.3e}")
+    assert after < 0.8 * zero

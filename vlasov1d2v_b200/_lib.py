@@ -26,7 +26,8 @@ EXPORTED = (
     "vl_rk_stage", "vl_run_state_init", "vl_ssp_rk3_steps", "vl_sync_ghosts",
     "vl_ssp_rk3_steps_noalloc", "vl_initial_state", "vl_smooth_edges", "vl_interpolate",
     "vl_set_background", "vl_ens_create", "vl_ens_destroy", "vl_ens_workspace_bytes", "vl_ens_bind",
-    "vl_ens_schedule", "vl_ens_commit", "vl_ens_steps",
+    "vl_ens_schedule", "vl_ens_commit", "vl_ens_steps", "vl_mlp_dims", "vl_mlp_forward",
+    "vl_mlp_partial_floats", "vl_mlp_backward", "vl_mlp_adam", "vl_closure_features", "vl_closure_apply",
 )
 NOALLOC_SCRATCH_BYTES = 1 << 20
 
@@ -108,6 +109,16 @@ def _declare(lib):
     lib.vl_ens_schedule.argtypes = [vp, i32, i32, i32]
     lib.vl_ens_commit.argtypes = [vp]
     lib.vl_ens_steps.argtypes = [vp, i32, vp]
+    f32, f64 = ctypes.c_float, ctypes.c_double
+    pi32 = ctypes.POINTER(i32)
+    lib.vl_mlp_dims.argtypes = [pi32, pi32, pi32, pi32, pi32]
+    lib.vl_mlp_forward.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.vl_mlp_partial_floats.argtypes = [i32]
+    lib.vl_mlp_partial_floats.restype = ctypes.c_size_t
+    lib.vl_mlp_backward.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.vl_mlp_adam.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, f32, vp]
+    lib.vl_closure_features.argtypes = [vp, i32, i32, i32, i32, vp, f64, f64, vp, vp, f64, f64, f64, vp, vp, vp]
+    lib.vl_closure_apply.argtypes = [vp, i32, i32, i32, i32, vp, vp, f64, f32, vp, f64, vp, vp]
     lib.vl_initial_state.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp,
                                      ctypes.c_double, vp]
     lib.vl_smooth_edges.argtypes = [vp, i32, i32, i32, i32, i32, vp]
@@ -115,7 +126,7 @@ def _declare(lib):
                                    i32, i32, i32, vp, vp]
     for name in EXPORTED:
         if name not in ("vl_last_error", "vl_abi_version", "vl_state_elems", "vl_workspace_bytes",
-                        "vl_ens_workspace_bytes"):
+                        "vl_ens_workspace_bytes", "vl_mlp_partial_floats"):
             getattr(lib, name).restype = i
 
 
