@@ -196,6 +196,24 @@ VL_API int vl_set_background(vl_ctx *ctx, const float *rb, const float *eu);
  * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */
 VL_API int vl_sync_ghosts(vl_ctx *ctx, void *f, void *stage, void *stream);
 
+/* ---- the DG Poisson solve and the linear SSP-RK stepper's interior update ------------------- */
+
+/* Elliptic.poisson (main/elliptic.py:85-115): stabilised central-flux DG solve of the
+ * mean-subtracted charge density.  inv_op = the inverse of the bordered operator
+ * [(nx n + 1)^2] (Elliptic.invert), mass = the element mass matrix [n][n], grad_op = the
+ * gradient operator [nx n][nx n] (G[q][p]), all device tables of the host set-up
+ * (main/elliptic.py:24-83); anti_alias != 0 filters the potential and the field through the
+ * context's high-order DFT.  Writes E[(nx+2)][n] (periodic ghosts) and phi[nx][n] (may be NULL).
+ * One CTA: nx n up to about 8000.                                                              */
+VL_API int vl_poisson_dg(vl_ctx *ctx, const double *charge_density, const double *inv_op,
+                         const double *mass, const double *grad_op, int32_t anti_alias, double *E,
+                         double *phi, void *stream);
+
+/* y[interior] <- alpha y[interior] + beta x[interior] (x may be NULL: beta ignored); ghost
+ * elements untouched.  The accumulation of Stepper.ssp_rk_update (main/timestep.py:195, :213). */
+VL_API int vl_axpby_interior(vl_ctx *ctx, void *y, const void *x, double alpha, double beta,
+                             void *stream);
+
 /* ---- around the loop: initial state, post-processing ------------------------------------------
  * These take the grid dimensions and state precision directly (no context): they need none of
  * the context's tables.  prec is VL_FP64 or VL_FP32; arithmetic is FP64 in both. */

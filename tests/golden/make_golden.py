@@ -187,6 +187,31 @@ def gen_cfg1(nsteps=200, out_name="cfg1_200", summary=True):
     np.savez_compressed(os.path.join(HERE, "cfg1_200.npz"), **out)
 
 
+def gen_linear(res=(4, 6, 5), order=4, nsteps=2):
+    """The DG central-flux Poisson solve (main/elliptic.py:24-115) of the initial density, and
+    steps of the linear SSP-RK3 stepper (main/timestep.py:189-229) that uses it."""
+    s = _setup(res, order)
+    grids, el, f = s["grids"], s["el"], s["f"]
+    el.build_central_flux_operator(grid=grids.x, basis=s["basis"].b1)
+    el.invert()
+    n0 = f.moment_zero()
+    el.poisson(charge_density=cp.mean(n0) - n0, grid=grids.x, basis=s["basis"].b1)
+    out = {"res": np.array(res), "order": order, "f_init": _np(f.arr), "rho_init": _np(n0),
+           "E_dg": _np(el.electric_field), "phi_dg": _np(el.potential)}
+    st = R.timestep.Stepper(time_order=3, space_order=order, write_time=1.0e9, final_time=1.0e9,
+                            linear=True)
+    st.adapt_time_step(max_speeds=R.timestep.get_max_speeds(grids, el, s["refs"]),
+                       dx=grids.x.dx, du=grids.u.dx, dv=grids.v.dx)
+    out["dt0"] = st.dt
+    for it in range(nsteps):
+        st.ssp_rk_update(distribution=f, basis=s["basis"], grids=grids, elliptic=el,
+                         dg_flux=s["flux"], refs=s["refs"])
+        out[f"f_step{it + 1}"] = _np(f.arr)
+        out[f"E_step{it + 1}"] = _np(el.electric_field)
+        out[f"dt_step{it + 1}"] = st.dt
+    np.savez_compressed(os.path.join(HERE, "linear.npz"), **out)
+
+
 def gen_post(res=(3, 3, 4), order=4, seed=5):
     """Post-processing operators of the reference on a random state: smooth_edges
     (main/grid.py:116-134) and Basis3D.interpolate_values (main/basis.py:291-317) on the
@@ -210,7 +235,7 @@ def gen_post(res=(3, 3, 4), order=4, seed=5):
 
 
 def main(argv):
-    which = argv or ["basis", "tiny", "small", "n8", "n9", "cfg1", "post"]
+    which = argv or ["basis", "tiny", "small", "n8", "n9", "cfg1", "post", "linear"]
     if "basis" in which:
         gen_basis()
     if "tiny" in which:
@@ -225,6 +250,8 @@ def main(argv):
         gen_cfg1()
     if "post" in which:
         gen_post()
+    if "linear" in which:
+        gen_linear()
     if "cfg1_noise" in which:
         # the same run with a different BLAS thread count: the reference's own summation-order
         # noise floor for the energy history (run with OPENBLAS_NUM_THREADS=1)

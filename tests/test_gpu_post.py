@@ -112,3 +112,34 @@ def test_checkpoint_resume_is_exact(cuda, tmp_path):
     np.testing.assert_array_equal(c.stepper.field_energy, a.stepper.field_energy)
     np.testing.assert_array_equal(c.stepper.time_array, a.stepper.time_array)
     assert c.stepper.steps_counter == a.stepper.steps_counter == 6
+
+
+def test_dg_poisson_and_linear_stepper_match_reference(cuda):
+    """Elliptic.poisson (central-flux DG with anti-aliasing) of the initial density and two steps
+    of the linear SSP-RK3 stepper, against the reference's fixture."""
+    from helpers import F_RTOL, field_rtol
+    from vlasov1d2v_b200 import problem
+    from vlasov1d2v_b200.timestep import Stepper, get_max_speeds
+
+    G = golden("linear")
+    res, n = tuple(int(r) for r in G["res"]), int(G["order"])
+    p = problem.build(res, n)
+    np.testing.assert_array_equal(p.f.arr.get(), G["f_init"])
+    el = p.elliptic
+    el.build_central_flux_operator(grid=p.grids.x, basis=p.basis.b1)
+    el.invert()
+    rho = p.f.moment_zero()
+    el.poisson(charge_density=rho.mean() - rho, grid=p.grids.x, basis=p.basis.b1)
+    tol = field_rtol(G["rho_init"])
+    assert rel_err(el.electric_field.get(), G["E_dg"]) < tol
+    assert rel_err(el.potential.get(), G["phi_dg"]) < tol
+    st = Stepper(time_order=3, space_order=n, write_time=1e9, final_time=1e9, linear=True)
+    st.adapt_time_step(get_max_speeds(p.grids, el, p.refs), p.grids.x.dx, p.grids.u.dx, p.grids.v.dx)
+    assert abs(st.dt - float(G["dt0"])) <= 1e-13 * float(G["dt0"])
+    for it in (1, 2):
+        st.ssp_rk_update(distribution=p.f, basis=p.basis, grids=p.grids, elliptic=el, dg_flux=p.flux,
+                         refs=p.refs)
+        inner = (slice(1, -1), slice(None), slice(1, -1), slice(None), slice(1, -1), slice(None))
+        assert rel_err(p.f.arr.get()[inner], G[f"f_step{it}"][inner]) < F_RTOL
+        assert rel_err(el.electric_field.get(), G[f"E_step{it}"]) < tol
+        assert abs(st.dt - float(G[f"dt_step{it}"])) <= 1e-12 * st.dt

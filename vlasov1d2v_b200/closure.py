@@ -133,8 +133,11 @@ class MLP:
         self.refresh_bf16()
 
 
-def train(mlp, X, T, epochs=10, batch=8192, lr=2e-3, seed=0, val=None, log=None):
-    """Adam on shuffled minibatches (all on the device); returns the loss history."""
+def train(mlp, X, T, epochs=10, batch=8192, lr=2e-3, seed=0, val=None, log=None, noise=0.0,
+          weight_decay=0.0):
+    """Adam on shuffled minibatches (all on the device); ``noise`` adds Gaussian noise of that
+    standard deviation to the state features of each minibatch (robustness of the closure to
+    states off the training manifold).  Returns the loss history."""
     n = X.shape[0]
     g = torch.Generator(device=X.device)
     g.manual_seed(seed)
@@ -148,10 +151,12 @@ def train(mlp, X, T, epochs=10, batch=8192, lr=2e-3, seed=0, val=None, log=None)
         for s in range(steps_per_epoch):
             idx = perm[s * batch:(s + 1) * batch]
             xb, tb = X[idx].contiguous(), T[idx].contiguous()
+            if noise > 0.0:
+                xb[:, :84] += noise * torch.randn(xb[:, :84].shape, device=xb.device, generator=g)
             Y = mlp.gradients(xb, tb, buf)
             # cosine learning-rate decay
             k = ep * steps_per_epoch + s
-            mlp.adam(lr * 0.5 * (1.0 + math.cos(math.pi * k / total)))
+            mlp.adam(lr * 0.5 * (1.0 + math.cos(math.pi * k / total)), weight_decay=weight_decay)
             if s % 16 == 0:
                 tot += float(((Y[:, :NOUT] - tb) ** 2).mean())
         rec = {"epoch": ep, "train_loss": tot / max((steps_per_epoch + 15) // 16, 1)}
@@ -357,10 +362,11 @@ class ClosureStepper:
         self._closure(sb, f, _RK[2][2])
         self.dt.copy_(self._hist[1, k:k + 1])
 
-    def run_steps(self, nsteps, batch=32, use_graph=True, growth_bound=1e6):
-        """Advance ``nsteps`` steps.  Fallback: a batch whose energy or dt is non-finite, or
-        whose energy exceeds ``growth_bound`` times the initial energy, is undone and the run
-        continues with the plain coarse operator (``fallback_step`` records where)."""
+    def run_steps(self, nsteps, batch=32, use_graph=True, max_rate=0.5):
+        """Advance ``nsteps`` steps.  Fallback: a batch whose energy or dt is non-finite, or in
+        which the field energy grows faster than exp(2 max_rate t) (far above the physical
+        growth rates of the cyclotron-harmonic instability), is undone and the run continues
+        with the plain coarse operator (``fallback_step`` records where)."""
         dev = self.f.device
         done = 0
         while done < nsteps:
@@ -372,7 +378,9 @@ class ClosureStepper:
             except FloatingPointError:
                 bad = True
             if not bad and self.mlp is not None:
-                bad = max(self.energies[snap[3]:]) > growth_bound * max(self.energies[0], 1e-300)
+                w0 = max(self.energies[snap[3] - 1], 1e-300)
+                dt_b = max(self.time - snap[2], 1e-300)
+                bad = max(self.energies[snap[3]:]) > w0 * math.exp(2.0 * max_rate * dt_b)
             if bad:
                 if self.mlp is None:
                     raise FloatingPointError("non-finite energy or dt in the plain coarse run")

@@ -73,6 +73,7 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--t-end", type=float, default=30.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--noise", type=float, default=0.02, help="feature noise during training")
     ap.add_argument("--fine-res", type=int, nargs=3, default=[16, 60, 60])
     ap.add_argument("--coarse-res", type=int, nargs=3, default=[16, 20, 20])
     args = ap.parse_args(argv)
@@ -109,7 +110,8 @@ def main(argv=None):
     zero = float((Tv ** 2).mean())
     _log({"samples": int(n), "data_s": out["data_s"], "val_loss_plain": zero})
     t1 = time.perf_counter()
-    hist = train(mlp, Xt, Tt, epochs=args.epochs, batch=8192, lr=2e-3, val=(Xv, Tv), log=_log)
+    hist = train(mlp, Xt, Tt, epochs=args.epochs, batch=8192, lr=2e-3, val=(Xv, Tv), log=_log,
+                 noise=args.noise, weight_decay=1e-4)
     torch.cuda.synchronize()
     out["train_s"] = time.perf_counter() - t1
     out["val_loss_plain"] = zero
@@ -122,6 +124,19 @@ def main(argv=None):
     out["fine_s"] = _timed(lambda: _run_to(fine, args.t_end))
     _, plain = _problems(q, fine_res, coarse_res)
     out["plain_s"] = _timed(lambda: _run_to(plain, args.t_end))
+    # the one-step RHS error of plain coarse vs closure on the held-out draw's fine states
+    Xh, Th = [], []
+    _, ch = _problems(q, fine_res, coarse_res)
+    fh, _ = _problems(q, fine_res, coarse_res)
+    for _ in range(4):
+        fh.stepper.run_steps(fh.f, fh.basis, fh.elliptic, fh.grids, fh.flux, fh.refs, args.every * 2)
+        x, t = make_pair(fh, ch, proj, escale)
+        Xh.append(x)
+        Th.append(t)
+    Xh, Th = torch.cat(Xh), torch.cat(Th)
+    out["held_out_rhs_err_plain"] = float((Th ** 2).mean())
+    out["held_out_rhs_err_closure"] = evaluate(mlp, Xh, Th)
+    del fh, ch
     _, cl = _problems(q, fine_res, coarse_res)
     cs = ClosureStepper(cl, mlp=mlp, escale=escale)
     nsteps = plain.stepper.steps_counter

@@ -64,24 +64,26 @@ class Elliptic:
                                                    device=_device.device()))
 
     def poisson(self, charge_density, grid, basis, anti_alias=True):
-        """DG central-flux Poisson solve (``main/elliptic.py:85-115``)."""
-        rho = _device.as_tensor(charge_density)
-        n = grid.res * grid.order
-        rhs = torch.zeros(n + 1, dtype=torch.float64, device=rho.device)
-        rhs[:-1] = (self.poisson_coefficient *
-                    torch.tensordot(rho, _device.plain(basis.d_mass), dims=([1], [1]))).flatten()
-        sol = torch.matmul(_device.plain(self.inv_op), rhs)[:-1] / (grid.J ** 2.0)
-        potential = sol.reshape(grid.res, grid.order)
-        if anti_alias:
-            potential = _device.plain(grid.sum_fourier(grid.fourier_basis(potential)))
-        E = torch.zeros((grid.res_ghosts, grid.order), dtype=torch.float64, device=rho.device)
-        E[1:-1, :] = -1.0 * (grid.J * torch.tensordot(_device.plain(self.gradient_operator),
-                                                      potential, dims=([0, 1], [0, 1])))
-        if anti_alias:
-            E[1:-1, :] = _device.plain(grid.sum_fourier(grid.fourier_basis(E[1:-1, :])))
-        E[0, :] = E[-2, :]
-        E[-1, :] = E[1, :]
-        self.potential = _device.wrap(potential)
+        """DG central-flux Poisson solve (``main/elliptic.py:85-115``): one native kernel
+        (``vl_poisson_dg``) over the operator tables of ``build_central_flux_operator`` /
+        ``invert``."""
+        import ctypes
+
+        from . import _lib
+
+        if self.inv_op is None or self.gradient_operator is None:
+            raise RuntimeError("call build_central_flux_operator(grid, basis) and invert() first")
+        rho = _device.as_tensor(charge_density).contiguous()
+        ctx = get_context(grid, kappa=self.poisson_coefficient)
+        E = torch.empty((grid.res_ghosts, grid.order), dtype=torch.float64, device=rho.device)
+        phi = torch.empty((grid.res, grid.order), dtype=torch.float64, device=rho.device)
+        mass = _device.plain(basis.d_mass).contiguous()
+        _lib.call("vl_poisson_dg", ctx.handle, ctypes.c_void_p(rho.data_ptr()),
+                  ctypes.c_void_p(_device.plain(self.inv_op).data_ptr()), ctypes.c_void_p(mass.data_ptr()),
+                  ctypes.c_void_p(_device.plain(self.gradient_operator).data_ptr()), int(bool(anti_alias)),
+                  ctypes.c_void_p(E.data_ptr()), ctypes.c_void_p(phi.data_ptr()),
+                  ctypes.c_void_p(_device.stream_handle()))
+        self.potential = _device.wrap(phi)
         self.electric_field = _device.wrap(E)
 
     # -- hot path ------------------------------------------------------------------------------------

@@ -317,6 +317,48 @@ class Stepper:
         elliptic.electric_field = _device.wrap(run.E.clone())
         elliptic.potential = _device.wrap(run.phi.clone())
 
+    def ssp_rk_update(self, distribution, basis, grids, elliptic, dg_flux, refs):
+        """One step of the linear SSP-RK stepper of any order (``main/timestep.py:189-229``),
+        with the DG central-flux Poisson solve (``Elliptic.poisson``) for every stage field:
+        acc = c0 f; copy <- copy + dt R(copy), acc += c_i copy (i = 1..order-1);
+        f = acc + c_last dt R(copy); dt adapted from the last field.  Device kernels throughout
+        (moment, ``vl_poisson_dg``, fused Euler stage, ``vl_axpby_interior``, RHS)."""
+        if self.dt is None:
+            raise ValueError("dt is not set (call adapt_time_step first)")
+        c = [float(v) for v in np.asarray(self.coefficients).ravel()]
+        f = _device.plain(distribution.arr)
+        ctx = self._context(distribution, elliptic, grids, refs)
+        key = (f.data_ptr(), tuple(f.shape), f.dtype)
+        if getattr(self, "_lin_key", None) != key:
+            self._lin = (torch.empty_like(f), torch.empty_like(f), torch.empty_like(f))
+            self._lin_key = key
+        A, B, R = self._lin
+        stream = ctypes.c_void_p(_device.stream_handle())
+        # periodic x ghosts of f; the copy (and the scratch) take all of f incl. ghosts
+        ctx.sync_ghosts(f, A)
+        ctx.sync_ghosts(f, B)
+        _lib.call("vl_axpby_interior", ctx.handle, ctypes.c_void_p(f.data_ptr()), None, c[0], 0.0, stream)
+        dt_t = torch.tensor([float(self.dt)], dtype=torch.float64, device=f.device)
+        rho = torch.empty((grids.x.res, grids.x.order), dtype=torch.float64, device=f.device)
+
+        def field(arr):
+            ctx.moment(arr, rho)
+            elliptic.poisson(charge_density=(rho.mean() - rho), grid=grids.x, basis=basis.b1)
+            return _device.plain(elliptic.electric_field)
+
+        for i in range(1, self.time_order):
+            E = field(A)
+            ctx.rk_stage(0, A, None, B, E, dt_t)          # B = A + dt R(A)
+            A, B = B, A
+            _lib.call("vl_axpby_interior", ctx.handle, ctypes.c_void_p(f.data_ptr()),
+                      ctypes.c_void_p(A.data_ptr()), 1.0, c[i], stream)
+        E = field(A)
+        ctx.rhs(A, E, R, xhalo=_lib.VL_XHALO_PERIODIC)
+        _lib.call("vl_axpby_interior", ctx.handle, ctypes.c_void_p(f.data_ptr()),
+                  ctypes.c_void_p(R.data_ptr()), 1.0, c[-1] * float(self.dt), stream)
+        self.adapt_time_step(max_speeds=get_max_speeds(grids, elliptic, refs),
+                             dx=grids.x.dx, du=grids.u.dx, dv=grids.v.dx)
+
     def adapt_time_step(self, max_speeds, dx, du, dv):
         self.dt = self.courant / ((max_speeds[0] / dx) + (max_speeds[1] / du) + (max_speeds[2] / dv))
 
