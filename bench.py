@@ -347,6 +347,13 @@ def measure_precision(precision, steps, warmup, reps, dist):
     }
 
 
+def replica_throughput(dist, ms, steps, dof):
+    """Whole-job throughput of independent replicas: the step time is the slowest rank's
+    (max over ranks of the device-timed region), the value the sum of every rank's DOF over it."""
+    ms_step = dist.max(ms) / steps
+    return ms_step, dist.sum(dof / (ms_step * 1e-3))
+
+
 class _NoDist:
     def barrier(self):
         pass
@@ -359,15 +366,16 @@ class _NoDist:
 
 
 class _TorchDist:
-    def __init__(self, torch, dist):
+    def __init__(self, torch, dist, device="cuda"):
         self.t = torch
         self.d = dist
+        self.device = device
 
     def barrier(self):
         self.d.barrier()
 
     def _reduce(self, x, op):
-        v = self.t.tensor([float(x)], dtype=self.t.float64, device="cuda")
+        v = self.t.tensor([float(x)], dtype=self.t.float64, device=self.device)
         self.d.all_reduce(v, op=op)
         return float(v.item())
 
@@ -432,8 +440,7 @@ def main():
     peak, peak_src = measured_peak_hbm()
     out = {}
     for prec, r in results.items():
-        ms_step = dist.max(r["ms"]) / r["steps"]
-        value = dist.sum(r["dof"] / (ms_step * 1e-3))
+        ms_step, value = replica_throughput(dist, r["ms"], r["steps"], r["dof"])
         stage_s = sum(r["stage_ms"]) * 1e-3
         achieved = sum(r["stage_bytes"]) / stage_s / 1e9
         ratio, tsrc = profiled_traffic_ratio(prec)
