@@ -185,7 +185,7 @@ VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, 
  *   r0 = E_i eu + rb,
  * with rb = J_u a B v D_u f0 + J_v (-a B u) D_v f0 and eu = J_u a D_u f0 precomputed in FP64
  * and stored as float in the velocity-slab layout [(nu+2)][n][(nv+2)][n] (device pointers,
- * 8-byte aligned, caller-owned, kept until the next call).  f0 is continuous across element
+ * 16-byte aligned, caller-owned, kept until the next call).  f0 is continuous across element
  * faces, so its upwind and downwind face traces agree and one D_u table serves both signs of
  * the u speed.  The x contraction of f0 is zero (f0 is constant in x).  Pass two NULLs to switch
  * the split off.  FP32 contexts only.                                                         */

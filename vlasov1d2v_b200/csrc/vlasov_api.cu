@@ -21,6 +21,7 @@
 #include "vlasov_stage.cuh"
 #include "vlasov_stage_tma.cuh"
 #include "vlasov_stage_frag.cuh"
+#include "vlasov_stage_gen.cuh"
 
 #include "vlasov_ctx.cuh"
 
@@ -116,6 +117,32 @@ int state_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     return VL_OK;
 }
 
+// 2-D view [U n][V n] of a background-split table (FP32), box (32, n): one tile's rows
+int bg_map(vl_ctx *c, const float *ptr, int n, CUtensorMap *out) {
+    auto key = std::make_pair(static_cast<const void *>(ptr), 8);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2;
+    cuuint64_t dims[2] = {V * n, U * n};
+    cuuint64_t strides[1] = {V * n * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)vl::FragGeom<float>::COLS, (cuuint32_t)n};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (background table) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
 template <int N, typename T>
 int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageTables<T> tb;
@@ -147,9 +174,26 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             if ((rc = state_map<N, T>(c, a.in, 1, &maps.in_xface))) return rc;
             if ((rc = state_map<N, T>(c, a.in, 2, &maps.in_uface))) return rc;
             if ((rc = state_map<N, T>(c, a.fn ? a.fn : a.in, 7, &maps.fn_tile))) return rc;
+            if (G::BG && a.bg_rb != nullptr) {
+                if ((rc = bg_map(c, a.bg_eu, N, &maps.bg_eu))) return rc;
+                if ((rc = bg_map(c, a.bg_rb, N, &maps.bg_rb))) return rc;
+            } else {
+                std::memset(&maps.bg_eu, 0, sizeof(maps.bg_eu));
+                std::memset(&maps.bg_rb, 0, sizeof(maps.bg_rb));
+            }
             vl::stage_frag_kernel<T><<<grid, G::THREADS, G::smem_bytes(), s>>>(a, tb, maps);
             return check_launch("stage_frag_kernel");
         }
+    }
+    if (c->stage_kernel == VL_STAGE_GEN) {
+        using G = vl::GenGeom<N, T>;
+        // pair copies and stores of even orders need pair-aligned buffers
+        const uintptr_t align = (N % 2 == 0) ? 2 * sizeof(T) : sizeof(T);
+        if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+             reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out)) % align)
+            return fail(VL_ERR_INVALID, "state buffers must be aligned to two elements");
+        vl::stage_gen_kernel<N, T><<<grid, G::THREADS, G::smem_bytes(), s>>>(a, tb);
+        return check_launch("stage_gen_kernel");
     }
     if constexpr (vl::TmaGeom<N, T>::SUPPORTED) {
         if (c->use_tma) {
@@ -192,8 +236,17 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag) {
+int stage_occupancy_t(bool tma, bool frag, bool gen) {
     int blocks = 0;
+    if (gen) {
+        using G = vl::GenGeom<N, T>;
+        const size_t smem = G::smem_bytes();
+        cudaFuncSetAttribute(vl::stage_gen_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_kernel<N, T>, G::THREADS, smem) !=
+            cudaSuccess)
+            return 1;
+        return blocks > 0 ? blocks : 1;
+    }
     if constexpr (N == 8) {
         if (frag) {
             using G = vl::FragGeom<T>;
@@ -237,18 +290,36 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag);
-        case 2: return stage_occupancy_t<2, T>(tma, frag);
-        case 3: return stage_occupancy_t<3, T>(tma, frag);
-        case 4: return stage_occupancy_t<4, T>(tma, frag);
-        case 5: return stage_occupancy_t<5, T>(tma, frag);
-        case 6: return stage_occupancy_t<6, T>(tma, frag);
-        case 7: return stage_occupancy_t<7, T>(tma, frag);
-        case 8: return stage_occupancy_t<8, T>(tma, frag);
-        case 9: return stage_occupancy_t<9, T>(tma, frag);
-        case 10: return stage_occupancy_t<10, T>(tma, frag);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen);
+        default: return 1;
+    }
+}
+
+// v elements per stage tile of the generic kernel
+template <typename T>
+int gen_ept(int n) {
+    switch (n) {
+        case 1: return vl::GenEpt<1, T>::value;
+        case 2: return vl::GenEpt<2, T>::value;
+        case 3: return vl::GenEpt<3, T>::value;
+        case 4: return vl::GenEpt<4, T>::value;
+        case 5: return vl::GenEpt<5, T>::value;
+        case 6: return vl::GenEpt<6, T>::value;
+        case 7: return vl::GenEpt<7, T>::value;
+        case 8: return vl::GenEpt<8, T>::value;
+        case 9: return vl::GenEpt<9, T>::value;
+        case 10: return vl::GenEpt<10, T>::value;
         default: return 1;
     }
 }
@@ -264,7 +335,12 @@ bool tma_supported(const vl_config &g) {
 }
 
 // v elements per tile of the stage kernel
-int stage_epw(int n) { return 32 / n; }   // 4 at n = 8 for both the TMA and fragment kernels
+// v elements per stage tile: 32 / n for the pencil, TMA and fragment kernels (4 at n = 8)
+int stage_epw(const vl_ctx *c) {
+    if (c->stage_kernel == VL_STAGE_GEN)
+        return c->cfg.precision == VL_FP64 ? gen_ept<double>(c->cfg.n) : gen_ept<float>(c->cfg.n);
+    return 32 / c->cfg.n;
+}
 
 // ------------------------------------------------------------------------------------------
 // moment kernel dispatch
@@ -506,9 +582,29 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         const char *env = getenv("VLASOV1D2V_NO_FRAG");
         if (env && env[0] == '1') c->use_frag = false;
     }
-    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma, c->use_frag)
-                                              : stage_occupancy<float>(n, c->use_tma, c->use_frag);
-    const int bt = stage_epw(n);
+    // stage kernel (fastest measured per order and precision): the fragment kernel for n = 8, the
+    // TMA kernel for the other aligned orders (n = 2, 4), then the asynchronous-copy kernel in FP64
+    // and the register-pencil kernel in FP32; VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects
+    // one for comparisons
+    c->stage_kernel = c->use_frag ? VL_STAGE_FRAG
+                    : c->use_tma  ? VL_STAGE_TMA
+                    : (cfg->precision == VL_FP64 ? VL_STAGE_GEN : VL_STAGE_PENCIL);
+    {
+        const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
+        if (env) {
+            const std::string k(env);
+            if (k == "gen") c->stage_kernel = VL_STAGE_GEN;
+            else if (k == "pencil") c->stage_kernel = VL_STAGE_PENCIL;
+            else if (k == "tma" && c->use_tma) c->stage_kernel = VL_STAGE_TMA;
+            else if (k == "frag" && c->use_frag) c->stage_kernel = VL_STAGE_FRAG;
+        }
+        c->use_frag = c->stage_kernel == VL_STAGE_FRAG;
+        if (c->stage_kernel != VL_STAGE_TMA && c->stage_kernel != VL_STAGE_FRAG) c->use_tma = false;
+    }
+    const bool gen = c->stage_kernel == VL_STAGE_GEN;
+    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen)
+                                              : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen);
+    const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double
     // the kernel time)
@@ -670,8 +766,8 @@ int vl_set_background(vl_ctx *c, const float *rb, const float *eu) {
     if ((rb == nullptr) != (eu == nullptr)) return fail(VL_ERR_INVALID, "background tables: give both or none");
     if (rb && c->cfg.precision != VL_FP32)
         return fail(VL_ERR_UNSUPPORTED, "the background split is a form of the FP32 context");
-    if ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(eu)) & 7)
-        return fail(VL_ERR_INVALID, "background tables must be 8-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(rb) | reinterpret_cast<uintptr_t>(eu)) & 15)
+        return fail(VL_ERR_INVALID, "background tables must be 16-byte aligned");
     c->bg_rb = rb;
     c->bg_eu = eu;
     return VL_OK;

@@ -11,6 +11,8 @@
 #include "vlasov1d2v.h"
 #include "vlasov_kernels.cuh"
 
+enum vl_stage_kernel { VL_STAGE_PENCIL = 0, VL_STAGE_TMA = 1, VL_STAGE_FRAG = 2, VL_STAGE_GEN = 3 };
+
 struct vl_ctx {
     vl_config cfg;      // scalars (pointer members cleared)
     int device;
@@ -33,6 +35,7 @@ struct vl_ctx {
     int *d_err = nullptr;         // device error word of operators run without a loop state
     bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
     bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
+    int stage_kernel = VL_STAGE_GEN;   // which stage kernel the launches use (vl_stage_kernel)
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
     const float *bg_eu = nullptr;
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer

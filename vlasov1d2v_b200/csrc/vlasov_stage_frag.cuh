@@ -8,7 +8,8 @@
 // outputs:
 //   x:  D[i][k] += sum_m up[i][m] F[m][j][k]       A = up (registers), B = tile plane rows
 //   v:  D[i][k] += sum_m F[i][j][m] up[k][m]       A = tile row slice, B = up^T (registers)
-// with the upwind lifts as a third k-chunk of each (two nonzero columns).  The u contraction
+// with the own-trace part of each upwind lift folded into the up fragments selected by the sign
+// of the speed (upP / upM) and the neighbour trace added by one FMA per output.  The u contraction
 // mixes the j of one thread's own outputs and runs on the FMA pipes from a per-thread copy of
 // F[i][0..7][k..k+1].  The FP32 form runs all three contractions on the FMA pipes in the
 // same layout.
@@ -20,6 +21,7 @@
 //   FN [i][9][34 | 36]   f^n (combination stages only)
 //   XF [side][j][32]     x upwind traces: (e-1, i = n-1) and (e+1, i = 0)
 //   UF [side][i][32]     u upwind traces: (a-1, j = n-1) and (a+1, j = 0)
+//   BG [table][j][32]    FP32 background split only: the eu and rb RHS tables of the tile
 // Two stages: tile q+1 streams in while tile q is computed.  Every wait is bounded: on timeout
 // the kernel raises bit 1 of the error word and returns.
 #pragma once
@@ -58,11 +60,15 @@ struct FragGeom {
     static constexpr size_t FN_B = al(sizeof(T) * (size_t)PSF * N);
     static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * COLS * N);
     static constexpr size_t UF_B = XF_B;
-    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B;
+    // background-split RHS tables (a form of the FP32 context only)
+    static constexpr bool BG = sizeof(T) == 4;
+    static constexpr size_t BG_B = BG ? al(sizeof(float) * (size_t)2 * COLS * N) : 0;
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B;
     static constexpr size_t smem_bytes() { return 2 * STAGE_B + 128; }
     static constexpr uint32_t TX_IN = sizeof(T) * W * ROWS * N;
     static constexpr uint32_t TX_FN = sizeof(T) * WF * ROWS * N;
     static constexpr uint32_t TX_FACE = sizeof(T) * COLS * N;
+    static constexpr uint32_t TX_BG = sizeof(float) * COLS * N;
 };
 
 struct FragMaps {
@@ -70,6 +76,8 @@ struct FragMaps {
     CUtensorMap in_xface;  // box (32, n, 1, 1, 1)
     CUtensorMap in_uface;  // box (32, 1, 1, n, 1)
     CUtensorMap fn_tile;   // box (WF, 9, 1, n, 1) over f^n
+    CUtensorMap bg_eu;     // box (32, n) over the [U n][V n] background tables (FP32 split)
+    CUtensorMap bg_rb;
 };
 
 // D[8x8] += A[8x4] B[4x8] in FP64 on the tensor cores; per lane (g = lane/4, t = lane%4):
@@ -130,7 +138,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     }
     const int kind = a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
-    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0);
+    const bool with_bg = G::BG && a.bg_rb != nullptr;
+    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0);
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile_cta = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -159,6 +168,11 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         tma_load_5d(uf, &maps.in_uface, &full[s], x0, N - 1, Ag - 1, 0, Eg);
         tma_load_5d(uf + sizeof(T) * COLS * N, &maps.in_uface, &full[s], x0, 0, Ag + 1, 0, Eg);
         if (with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
+        if (with_bg) {
+            unsigned char *bg = uf + G::UF_B;
+            tma_load_2d(bg, &maps.bg_eu, &full[s], x0, Ag * N);
+            tma_load_2d(bg + sizeof(float) * COLS * N, &maps.bg_rb, &full[s], x0, Ag * N);
+        }
     };
     if (tid == 0) {
         if (ntile_cta > 0) issue(0, 0);
@@ -171,13 +185,24 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
     const double Ei = a.E[Eg * N + g];
     // per-thread coefficients (runtime rows g and 2t, 2t + 1 of the tables)
-    T ca0, ca1, calift;            // MMA: up[g][t], up[g][4 + t], lift column t of row g
+    // MMA form: fragments up[g][t], up[g][4 + t] and their upwind-folded variants (speed >= 0
+    // folds the own right trace into column n-1, speed < 0 the own left trace into column 0), so
+    // only the neighbour trace remains as a lift: xi[g][0] (x, from the left) / -xi[g][1] (x, from
+    // the right) for the x direction, xi[k][0] / -xi[k][1] of the thread's columns k for v
+    T ca0, ca1, ca0M, ca1P, xil, xir, vil0, vil1, vir0, vir1;
     T upi[N], upk0[N], upk1[N];    // FMA form: up[g][.], up[2t][.], up[2t + 1][.]
     T xig0, xig1, xik00, xik01, xik10, xik11;
     if constexpr (G::MMA) {
         ca0 = tb.up[g * N + t];
         ca1 = tb.up[g * N + 4 + t];
-        calift = (t == 0) ? tb.xi[2 * g] : ((t == 1) ? -tb.xi[2 * g + 1] : (T)0);
+        ca0M = tb.upM[g * N + t];
+        ca1P = tb.upP[g * N + 4 + t];
+        xil = tb.xi[2 * g];
+        xir = -tb.xi[2 * g + 1];
+        vil0 = tb.xi[4 * t];
+        vil1 = tb.xi[4 * t + 2];
+        vir0 = -tb.xi[4 * t + 1];
+        vir1 = -tb.xi[4 * t + 3];
     } else {
 #pragma unroll
         for (int m = 0; m < N; ++m) {
@@ -218,11 +243,13 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const T *sFn = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B);
         const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
         const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
+        const float *sBG = reinterpret_cast<const float *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B);
 
         if (act) {
             const double sd0 = accel * (Ei + bfield * vn0);
             const double sd1 = accel * (Ei + bfield * vn1);
             const T sp0 = (T)sd0, sp1 = (T)sd1;
+            const T spu0 = sp0 * ju, spu1 = sp1 * ju;
             // F[g][m][cl..cl+1] for the u contraction, and the u upwind traces
             const T *pg = sIn + g * PS + P + cl;
             V2 fu[N];
@@ -243,31 +270,29 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                 const bool vpos = svd >= 0.0;
                 T dx0, dx1, dv0, dv1;
                 if constexpr (G::MMA) {
-                    // x: B rows m = t, 4 + t at column wc + g; lift rows xL (t = 0), xR (t = 1)
+                    // x: A = upwind-folded up (rows g), B rows m = t, 4 + t at column wc + g, then
+                    // the neighbour trace of the thread's columns
                     const T *pb = sIn + j * W + P + wc + g;
                     const T b0v = pb[t * PS];
                     const T b1v = pb[(4 + t) * PS];
-                    const T *pxl = xpos ? (sXF + j * COLS + wc + g) : pb;
-                    const T *pxr = xpos ? (pb + (N - 1) * PS) : (sXF + N * COLS + j * COLS + wc + g);
-                    const T blv = (t < 2) ? *((t == 0) ? pxl : pxr) : (T)0;
                     double x0 = 0.0, x1 = 0.0;
-                    dmma_8x8x4(x0, x1, ca0, b0v);
-                    dmma_8x8x4(x0, x1, ca1, b1v);
-                    dmma_8x8x4(x0, x1, calift, blv);
-                    // v: A = F[g][j][wc + 4c + t]; lift columns tL (t = 0), tR (t = 1)
+                    dmma_8x8x4(x0, x1, xpos ? ca0 : ca0M, b0v);
+                    dmma_8x8x4(x0, x1, xpos ? ca1P : ca1, b1v);
+                    const V2 xn = *reinterpret_cast<const V2 *>(sXF + (xpos ? 0 : N * COLS) + j * COLS + cl);
+                    const T xcn = xpos ? xil : xir;
+                    dx0 = fma(xcn, xn.x, x0);
+                    dx1 = fma(xcn, xn.y, x1);
+                    // v: A = F[g][j][wc + 4c + t], B = upwind-folded up^T, then the neighbour
+                    // element's trace at row (g, j)
                     const T *pa = prow + j * W;
                     const T a0v = pa[t];
                     const T a1v = pa[4 + t];
-                    const int toff = (t == 0) ? (vpos ? -1 : 0) : (vpos ? N - 1 : N);
-                    const T alv = (t < 2) ? pa[toff] : (T)0;
                     double v0 = 0.0, v1 = 0.0;
-                    dmma_8x8x4(v0, v1, a0v, ca0);
-                    dmma_8x8x4(v0, v1, a1v, ca1);
-                    dmma_8x8x4(v0, v1, alv, calift);
-                    dx0 = x0;
-                    dx1 = x1;
-                    dv0 = v0;
-                    dv1 = v1;
+                    dmma_8x8x4(v0, v1, a0v, vpos ? ca0 : ca0M);
+                    dmma_8x8x4(v0, v1, a1v, vpos ? ca1P : ca1);
+                    const T vn = vpos ? pa[-1] : pa[N];
+                    dv0 = fma(vpos ? vil0 : vir0, vn, v0);
+                    dv1 = fma(vpos ? vil1 : vir1, vn, v1);
                 } else {
                     const T *pc = sIn + j * W + P + cl;   // F[m][j][cl..cl+1] at m = 0
                     dx0 = (T)0;
@@ -317,13 +342,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                 du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
                 du1 = fma(tb.xi[2 * j], uL1, du1);
                 du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
-                const T uxT = (T)uxd, svT = (T)svd;
-                T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
-                T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
-                if (a.bg_rb != nullptr) {   // RHS of the x-independent background
-                    const int vi = Ag * sA + j * sJ + col;
-                    const float2 eu = *reinterpret_cast<const float2 *>(a.bg_eu + vi);
-                    const float2 rb = *reinterpret_cast<const float2 *>(a.bg_rb + vi);
+                const T uxj = (T)uxd * jx, svj = (T)svd * jv;
+                T r0 = fma(uxj, dx0, fma(spu0, du0, svj * dv0));
+                T r1 = fma(uxj, dx1, fma(spu1, du1, svj * dv1));
+                if (with_bg) {   // RHS of the x-independent background (staged with the tile)
+                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * COLS + cl);
+                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + N * COLS + j * COLS + cl);
                     r0 += (T)fmaf((float)Ei, eu.x, rb.x);
                     r1 += (T)fmaf((float)Ei, eu.y, rb.y);
                 }

@@ -1,0 +1,477 @@
+// Fused SSP-RK stage kernel for every LGL order (sm_100a): asynchronous-copy pipelined tiles in
+// the (x node, column pair) layout.
+//
+// Tile = (x element e, u element a, EPT consecutive v elements).  Thread "item" (b, i, p) owns
+// x node i and the column pair k = 2p, 2p + 1 of tile element b, for all n values of j (for odd n
+// the second column of the last pair is a pad column that is computed but never stored).  Per j:
+//   x:  sum_m up[i][m] F[m][j][k]     n pair loads from the tile (shared across the items of
+//                                     one column pair: broadcast within a warp)
+//   v:  sum_m F[i][j][m] up[k][m]     the element's k-line (pair loads, shared by its pairs)
+//   u:  sum_m up[j][m] F[i][m][k]     from the thread's register copy of F[i][0..n-1][k, k+1];
+//                                     compile-time j, so up[j][m] is a constant-bank operand
+// plus the upwind lifts in the three directions, the flux speeds, the Jacobian-weighted sum, the
+// RK combination, the store, the periodic x-ghost refresh (stage 1 on f) and the zeroth-moment
+// partials of the result: the same fused operator as the n = 8 fragment kernel.
+//
+// Shared-memory stage (filled by cp.async, NST stages in flight; every thread copies a share of
+// each array, one warp per row, and the stage is published by cp.async.wait_group +
+// __syncthreads, so no wait can spin):
+//   IN [i][j][W]      stage input: tile columns at H + b SL + k (SL = n rounded up to even, one
+//                     pad column per element for odd n so that every pair is vector-aligned),
+//                     the left v trace of the tile at LH, the right one at H + nb SL
+//   FN [i][j][WN]     f^n (combination stages)
+//   XF [side][j][WF]  x upwind traces: (e-1, i = n-1) and (e+1, i = 0)
+//   UF [side][i][WF]  u upwind traces: (a-1, j = n-1) and (a+1, j = 0)
+//   BG [table][j][WF] FP32 background split: the eu and rb RHS tables of the tile
+//   UX [j]            u node coordinates of the tile's u element
+// W and WN are padded so that the k-line loads of the up-to-eight x nodes met by one warp fall
+// in distinct banks (searched at compile time for the actual lane assignment).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vlasov_kernels.cuh"
+
+namespace vl {
+
+__device__ __forceinline__ uint32_t gen_smem_addr(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(gen_smem_addr(dst)), "l"(src), "n"(BYTES)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(K) : "memory"); }
+
+// v elements per tile (both precisions fill 128-320 threads at >= 84% lane use; FP64 tiles are
+// kept small enough for two CTAs per SM)
+template <int N, typename T>
+struct GenEpt {
+    static constexpr int value = sizeof(T) == 8
+        ? (N == 1 ? 128 : N == 2 ? 64 : N == 3 ? 21 : N == 4 ? 16 : N == 5 ? 8 : N == 6 ? 7 : N == 7 ? 4 : N == 8 ? 4 : 3)
+        : (N == 1 ? 128 : N == 2 ? 64 : N == 3 ? 21 : N == 4 ? 16 : N == 5 ? 8 : N == 6 ? 7 : N == 7 ? 8 : N == 8 ? 8 : 5);
+};
+
+// shared-memory wavefronts of one warp-wide pair load at element address
+// plane * i + SL * b (+ 2 p when with_p): 64-bit accesses in half-warp phases, 128-bit in quarter-warps
+template <int N, int EPT, int NT, int ES>
+constexpr int gen_load_cost(int plane, bool with_p) {
+    constexpr int P = (N + 1) / 2, SL = N + (N & 1), ITEMS = EPT * N * P;
+    const int words = 2 * ES / 4;            // 4-byte words per lane
+    const int phase = 32 / words;            // lanes per phase
+    int total = 0;
+    for (int w = 0; w < (ITEMS + 31) / 32; ++w) {
+        for (int ph = 0; ph < 32; ph += phase) {
+            int cnt[32] = {};
+            long addr[32] = {};
+            int na = 0;
+            for (int l = ph; l < ph + phase; ++l) {
+                const int it = 32 * w + l;
+                if (it >= ITEMS) continue;
+                const int p = it % P, bi = it / P, i = bi % N, b = bi / N;
+                const long a = (long)plane * i + (long)SL * b + (with_p ? 2 * p : 0);
+                bool seen = false;
+                for (int q = 0; q < na; ++q) seen = seen || (addr[q] == a);
+                if (seen) continue;
+                addr[na++] = a;
+                const long w0 = a * (ES / 4);
+                for (int k = 0; k < words; ++k) ++cnt[(int)((w0 + k) % 32)];
+            }
+            int mx = 1;
+            for (int k = 0; k < 32; ++k) mx = cnt[k] > mx ? cnt[k] : mx;
+            total += mx;
+        }
+    }
+    return total;
+}
+
+// smallest even row length in [w0, w0 + span) whose plane stride (n rows) minimises the load
+// wavefronts
+template <int N, int EPT, int NT, int ES>
+constexpr int gen_pick_row(int w0, bool with_p, int span) {
+    int best = w0, best_cost = 1 << 30;
+    for (int w = w0; w < w0 + span; w += 2) {
+        const int c = gen_load_cost<N, EPT, NT, ES>(N * w, with_p);
+        if (c < best_cost) {
+            best_cost = c;
+            best = w;
+        }
+    }
+    return best;
+}
+
+template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
+struct GenGeom {
+    static constexpr int EPT = EPT_;
+    static constexpr int P = (N + 1) / 2;           // column pairs per element
+    static constexpr int SL = N + (N & 1);          // element slot width (even)
+    static constexpr int H = 2;                     // first tile column of IN rows
+    static constexpr int LH = H - 1 - (SL - N);     // left v trace column: slot -1, node n-1
+    static constexpr int ITEMS = EPT * N * P;
+    static constexpr int THREADS = (ITEMS + 31) / 32 * 32;
+    static constexpr int NW = THREADS / 32;
+    static constexpr int WF = EPT * SL;             // face / background row length
+    static constexpr int W = gen_pick_row<N, EPT, THREADS, (int)sizeof(T)>(H + EPT * SL + 2, false, 16);
+    static constexpr int WN = gen_pick_row<N, EPT, THREADS, (int)sizeof(T)>(WF, true, 8);
+    static constexpr int PS = N * W;                // IN plane (x node) stride
+    static constexpr int PSF = N * WN;              // FN plane stride
+    static constexpr int NST = 2;                   // pipeline stages
+    static constexpr bool BG = sizeof(T) == 4;      // background split: FP32 contexts only
+    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
+    static constexpr size_t IN_B = al(sizeof(T) * (size_t)N * PS);
+    static constexpr size_t FN_B = al(sizeof(T) * (size_t)N * PSF);
+    static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * N * WF);
+    static constexpr size_t UF_B = XF_B;
+    static constexpr size_t BG_B = BG ? al(sizeof(float) * (size_t)2 * N * WF) : 0;
+    static constexpr size_t UX_B = al(sizeof(double) * (size_t)N);
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
+    static constexpr size_t smem_bytes() {
+        const size_t s = NST * STAGE_B;
+        const size_t red = sizeof(dd) * (size_t)THREADS;
+        return (s > red ? s : red) + 128;
+    }
+    // resident CTAs per SM the register allocation is sized for (shared memory permitting, and at
+    // least 128 / 168 registers per thread in FP32 / FP64; warps are allocated in pairs)
+    static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
+    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * (sizeof(T) == 8 ? 168 : 128));
+    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
+    static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
+    static_assert(ITEMS <= THREADS, "items exceed threads");
+};
+
+template <typename T>
+struct GenPair;
+template <>
+struct GenPair<double> {
+    using V = double2;
+};
+template <>
+struct GenPair<float> {
+    using V = float2;
+};
+
+// One CTA's share of a stage: x element e, tiles g, g + G, ... of that slab; writes the moment
+// partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
+// wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
+// tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
+template <int N, typename T, int EPT, typename TB>
+__device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
+                                               int g, int G, unsigned char *smem) {
+    using GG = GenGeom<N, T, EPT>;
+    using V2 = typename GenPair<T>::V;
+    constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
+    constexpr int PS = GG::PS, PSF = GG::PSF, NST = GG::NST, NW = GG::NW, NT = GG::THREADS;
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const bool has_item = tid < GG::ITEMS;
+    const int item = has_item ? tid : 0;
+    const int p = item % P;
+    const int bi = item / P;
+    const int i = bi % N;
+    const int b = bi / N;
+    const int cs = b * SL + 2 * p;                  // tile column of the pair (slot layout)
+    const int k0 = 2 * p;
+    const bool pad1 = (2 * p + 1) >= N;             // second column is the odd-order pad
+    const int k1 = pad1 ? N - 1 : 2 * p + 1;
+
+    const T *__restrict__ in = static_cast<const T *>(a.in);
+    const T *__restrict__ fn = static_cast<const T *>(a.fn);
+    T *out = static_cast<T *>(a.out);
+    T *gout = static_cast<T *>(a.ghost_out);
+    const int nx = a.nx, nu = a.nu, nv = a.nv;
+    const int U = nu + 2, V = nv + 2;
+    const int sJ = V * N, sA = sJ * N, sI = sA * U;
+    const size_t sE_ = (size_t)sI * N;
+    const int Eg = e + 1;
+    int El, Er;
+    if (a.xhalo == VL_XHALO_PERIODIC) {
+        El = (e == 0) ? nx : e;
+        Er = (e == nx - 1) ? 1 : e + 2;
+    } else {
+        El = e;
+        Er = e + 2;
+    }
+    const int kind = a.kind;
+    const bool with_fn = (kind == KIND_COMBINE);
+    const bool with_bg = GG::BG && a.bg_rb != nullptr;
+    const int nbt = (nv + EPT - 1) / EPT;
+    const int tiles = nu * nbt;
+    const int ntile = (g < tiles) ? (tiles - 1 - g) / G + 1 : 0;
+
+    // pad columns are never written by the copies: zero them once so that the pad outputs
+    // (computed, not stored) stay finite
+    {
+        uint4 *z = reinterpret_cast<uint4 *>(smem);
+        const int nz = (int)(NST * GG::STAGE_B / 16);
+        for (int q = tid; q < nz; q += blockDim.x) z[q] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    __syncthreads();
+
+    auto stage_ptr = [&](int s) { return smem + (size_t)s * GG::STAGE_B; };
+    // one row of ncol tile columns: global run -> slot layout
+    auto copy_row = [&](T *dst, const T *src, int ncol) {
+        if constexpr (N % 2 == 0) {
+            for (int c = 2 * lane; c < ncol; c += 64) cp_async<2 * sizeof(T)>(dst + c, src + c);
+        } else {
+            for (int c = lane; c < ncol; c += 32) cp_async<sizeof(T)>(dst + (c / N) * SL + c % N, src + c);
+        }
+    };
+    auto copy_row_f = [&](float *dst, const float *src, int ncol) {
+        if constexpr (N % 2 == 0) {
+            for (int c = 2 * lane; c < ncol; c += 64) cp_async<8>(dst + c, src + c);
+        } else {
+            for (int c = lane; c < ncol; c += 32) cp_async<4>(dst + (c / N) * SL + c % N, src + c);
+        }
+    };
+    auto issue = [&](int s, int tt) {
+        const int au = tt / nbt;
+        const int b0 = (tt - au * nbt) * EPT;
+        const int nb = min(EPT, nv - b0);
+        const int Ag = au + 1;
+        const int ncol = nb * N;
+        const size_t gc0 = (size_t)(b0 + 1) * N;
+        unsigned char *st = stage_ptr(s);
+        T *dIn = reinterpret_cast<T *>(st);
+        T *dFn = reinterpret_cast<T *>(st + GG::IN_B);
+        T *dXF = reinterpret_cast<T *>(st + GG::IN_B + GG::FN_B);
+        T *dUF = reinterpret_cast<T *>(st + GG::IN_B + GG::FN_B + GG::XF_B);
+        float *dBG = reinterpret_cast<float *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B);
+        double *dUX = reinterpret_cast<double *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B + GG::BG_B);
+        const T *slab = in + (size_t)Eg * sE_ + (size_t)Ag * sA + gc0;
+        for (int r = warp; r < N * N; r += NW) {
+            const int ii = r / N, jj = r - ii * N;
+            const T *src = slab + (size_t)ii * sI + (size_t)jj * sJ;
+            T *dst = dIn + ii * PS + jj * W + H;
+            copy_row(dst, src, ncol);
+            if (lane == 0) cp_async<sizeof(T)>(dst + (LH - H), src - 1);       // left v trace
+            if (lane == 1) cp_async<sizeof(T)>(dst + nb * SL, src + ncol);     // right v trace
+        }
+        if (with_fn) {
+            const T *fslab = fn + (size_t)Eg * sE_ + (size_t)Ag * sA + gc0;
+            for (int r = warp; r < N * N; r += NW) {
+                const int ii = r / N, jj = r - ii * N;
+                copy_row(dFn + ii * PSF + jj * WN, fslab + (size_t)ii * sI + (size_t)jj * sJ, ncol);
+            }
+        }
+        for (int r = warp; r < 4 * N; r += NW) {
+            const int side = (r / N) & 1, q = r % N;
+            const T *src;
+            T *dst;
+            if (r < 2 * N) {   // x traces: row j = q of (El, i = n-1) / (Er, i = 0)
+                src = in + (size_t)(side ? Er : El) * sE_ + (size_t)(side ? 0 : N - 1) * sI + (size_t)Ag * sA +
+                      (size_t)q * sJ + gc0;
+                dst = dXF + (side * N + q) * WF;
+            } else {           // u traces: row i = q of (a-1, j = n-1) / (a+1, j = 0)
+                src = in + (size_t)Eg * sE_ + (size_t)q * sI + (size_t)(side ? Ag + 1 : Ag - 1) * sA +
+                      (size_t)(side ? 0 : N - 1) * sJ + gc0;
+                dst = dUF + (side * N + q) * WF;
+            }
+            copy_row(dst, src, ncol);
+        }
+        if (with_bg) {
+            for (int r = warp; r < 2 * N; r += NW) {
+                const int tbl = r / N, jj = r % N;
+                const float *src = (tbl ? a.bg_rb : a.bg_eu) + (size_t)Ag * sA + (size_t)jj * sJ + gc0;
+                copy_row_f(dBG + (tbl * N + jj) * WF, src, ncol);
+            }
+        }
+        if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
+    };
+
+    const double accel = a.accel, bfield = a.bfield, nbfield = -a.bfield;
+    const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
+    const T dtT = (T)dtd, c0 = (T)a.c0, c1 = (T)a.c1, c2dt = (T)(a.c2 * dtd);
+    const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
+    const double Ei = a.E[Eg * N + i];
+    T upi[N], upk0[N], upk1[N];
+#pragma unroll
+    for (int m = 0; m < N; ++m) {
+        upi[m] = tb.up[i * N + m];
+        upk0[m] = tb.up[k0 * N + m];
+        upk1[m] = tb.up[k1 * N + m];
+    }
+    const T xig0 = tb.xi[2 * i], xig1 = tb.xi[2 * i + 1];
+    const T xik00 = tb.xi[2 * k0], xik01 = tb.xi[2 * k0 + 1];
+    const T xik10 = tb.xi[2 * k1], xik11 = tb.xi[2 * k1 + 1];
+    const double wf0 = wfin[k0], wf1 = pad1 ? 0.0 : wfin[k1];
+    double mk0 = 0.0, mk1 = 0.0;   // sum_j wu_j out[.., j, k] for the two columns
+
+#pragma unroll
+    for (int s0 = 0; s0 < NST - 1; ++s0) {
+        if (s0 < ntile) issue(s0, g + s0 * G);
+        cp_async_commit();
+    }
+    for (int q = 0; q < ntile; ++q) {
+        const int qn = q + NST - 1;
+        if (qn < ntile) issue(qn % NST, g + qn * G);
+        cp_async_commit();
+        const int tt = g + q * G;
+        const int au = tt / nbt;
+        const int b0 = (tt - au * nbt) * EPT;
+        const int nb = min(EPT, nv - b0);
+        const int Ag = au + 1;
+        const bool act = has_item && b < nb;
+        const int col = (b0 + b + 1) * N + 2 * p;    // global v-node column of the pair
+        const double vn0 = act ? a.v_nodes[col] : 0.0, vn1 = act ? a.v_nodes[col + 1] : 0.0;
+        cp_async_wait<NST - 1>();
+        __syncthreads();   // tile q visible to every thread
+        const unsigned char *st = stage_ptr(q % NST);
+        const T *sIn = reinterpret_cast<const T *>(st);
+        const T *sFn = reinterpret_cast<const T *>(st + GG::IN_B);
+        const T *sXF = reinterpret_cast<const T *>(st + GG::IN_B + GG::FN_B);
+        const T *sUF = reinterpret_cast<const T *>(st + GG::IN_B + GG::FN_B + GG::XF_B);
+        const float *sBG = reinterpret_cast<const float *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B);
+        const double *sUX =
+            reinterpret_cast<const double *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B + GG::BG_B);
+        if (act) {
+            const double sd0 = accel * (Ei + bfield * vn0);
+            const double sd1 = accel * (Ei + bfield * vn1);
+            const T sp0 = (T)sd0, sp1 = (T)sd1;
+            V2 fu[N];
+#pragma unroll
+            for (int m = 0; m < N; ++m) fu[m] = *reinterpret_cast<const V2 *>(sIn + i * PS + m * W + H + cs);
+            const V2 ufl = *reinterpret_cast<const V2 *>(sUF + i * WF + cs);
+            const V2 ufr = *reinterpret_cast<const V2 *>(sUF + (N + i) * WF + cs);
+            const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
+            const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
+            T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
+            const T *prow = sIn + i * PS + H + b * SL;   // k-line of element b at j = 0
+#pragma unroll
+            for (int j = 0; j < N; ++j) {
+                const double uxd = sUX[j];
+                const double svd = accel * (nbfield * uxd);
+                const bool xpos = uxd >= 0.0;
+                const bool vpos = svd >= 0.0;
+                // x: sum_m up[i][m] F[m][j][k] + lifts
+                const T *pc = sIn + j * W + H + cs;
+                T dx0 = (T)0, dx1 = (T)0;
+                V2 cm0, cmL;
+#pragma unroll
+                for (int m = 0; m < N; ++m) {
+                    const V2 cv = *reinterpret_cast<const V2 *>(pc + m * PS);
+                    if (m == 0) cm0 = cv;
+                    if (m == N - 1) cmL = cv;
+                    dx0 = fma(upi[m], cv.x, dx0);
+                    dx1 = fma(upi[m], cv.y, dx1);
+                }
+                const V2 xf0 = *reinterpret_cast<const V2 *>(sXF + j * WF + cs);
+                const V2 xf1 = *reinterpret_cast<const V2 *>(sXF + (N + j) * WF + cs);
+                const V2 xl = xpos ? xf0 : cm0;
+                const V2 xr = xpos ? cmL : xf1;
+                dx0 = fma(xig0, xl.x, dx0);
+                dx0 = fma(-xig1, xr.x, dx0);
+                dx1 = fma(xig0, xl.y, dx1);
+                dx1 = fma(-xig1, xr.y, dx1);
+                // v: sum_m F[i][j][m] up[k][m] + lifts (the element's k-line)
+                const T *pa = prow + j * W;
+                T line[2 * P];
+#pragma unroll
+                for (int m2 = 0; m2 < P; ++m2) {
+                    const V2 l2 = *reinterpret_cast<const V2 *>(pa + 2 * m2);
+                    line[2 * m2] = l2.x;
+                    line[2 * m2 + 1] = l2.y;
+                }
+                T dv0 = (T)0, dv1 = (T)0;
+#pragma unroll
+                for (int m = 0; m < N; ++m) {
+                    dv0 = fma(upk0[m], line[m], dv0);
+                    dv1 = fma(upk1[m], line[m], dv1);
+                }
+                const T tl = vpos ? pa[LH - H] : line[0];
+                const T tr = vpos ? line[N - 1] : pa[SL];
+                dv0 = fma(xik00, tl, dv0);
+                dv0 = fma(-xik01, tr, dv0);
+                dv1 = fma(xik10, tl, dv1);
+                dv1 = fma(-xik11, tr, dv1);
+                // u: sum_m up[j][m] F[i][m][k] + lifts (compile-time j: table constants)
+                T du0 = (T)0, du1 = (T)0;
+#pragma unroll
+                for (int m = 0; m < N; ++m) {
+                    du0 = fma(tb.up[j * N + m], fu[m].x, du0);
+                    du1 = fma(tb.up[j * N + m], fu[m].y, du1);
+                }
+                du0 = fma(tb.xi[2 * j], uL0, du0);
+                du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
+                du1 = fma(tb.xi[2 * j], uL1, du1);
+                du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
+                const T uxT = (T)uxd, svT = (T)svd;
+                T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
+                T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
+                if (with_bg) {   // RHS of the x-independent background
+                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * WF + cs);
+                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + (N + j) * WF + cs);
+                    r0 += (T)fmaf((float)Ei, eu.x, rb.x);
+                    r1 += (T)fmaf((float)Ei, eu.y, rb.y);
+                }
+                const V2 fij = fu[j];
+                V2 o;
+                if (kind == KIND_RHS) {
+                    o.x = r0;
+                    o.y = r1;
+                } else if (kind == KIND_EULER) {
+                    o.x = fma(dtT, r0, fij.x);
+                    o.y = fma(dtT, r1, fij.y);
+                } else {
+                    const V2 fnv = *reinterpret_cast<const V2 *>(sFn + i * PSF + j * WN + cs);
+                    o.x = fma(c2dt, r0, fma(c1, fij.x, c0 * fnv.x));
+                    o.y = fma(c2dt, r1, fma(c1, fij.y, c0 * fnv.y));
+                }
+                T *po = pout + (size_t)j * sJ;
+                if constexpr (N % 2 == 0) {
+                    *reinterpret_cast<V2 *>(po) = o;
+                } else {
+                    po[0] = o.x;
+                    if (!pad1) po[1] = o.y;
+                }
+                if (gout != nullptr) {
+                    // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
+                    const size_t gb = (size_t)i * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
+                    if (e == nx - 1) {
+                        gout[gb] = fij.x;
+                        if (!pad1) gout[gb + 1] = fij.y;
+                    }
+                    if (e == 0) {
+                        gout[(size_t)(nx + 1) * sE_ + gb] = fij.x;
+                        if (!pad1) gout[(size_t)(nx + 1) * sE_ + gb + 1] = fij.y;
+                    }
+                }
+                mk0 = fma(tb.wu[j], (double)o.x, mk0);
+                mk1 = fma(tb.wu[j], (double)o.y, mk1);
+            }
+        }
+        __syncthreads();   // stage q % NST consumed before it is refilled
+    }
+    cp_async_wait<0>();
+
+    if (a.partials == nullptr) return;
+    // moment partial of x node i: sum over the CTA's items of that node, fixed order
+    __syncthreads();
+    dd *sRed = reinterpret_cast<dd *>(smem);
+    sRed[tid] = has_item ? two_sum(wf0 * mk0, wf1 * mk1) : dd{0.0, 0.0};
+    __syncthreads();
+    if (tid < N) {
+        dd s = {0.0, 0.0};
+        for (int bb = 0; bb < EPT; ++bb)
+            for (int pp = 0; pp < P; ++pp) s = dd_add(s, sRed[(bb * N + tid) * P + pp]);
+        a.partials[((size_t)e * G + g) * N + tid] = s.hi + s.lo;
+    }
+    (void)NT;
+}
+
+template <int N, typename T>
+__global__ void __launch_bounds__(GenGeom<N, T>::THREADS, GenGeom<N, T>::MINB)
+stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
+    if (a.state != nullptr && a.state->active == 0) return;
+    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
+    gen_stage_body<N, T, GenGeom<N, T>::EPT>(a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
+}
+
+}  // namespace vl
