@@ -1,8 +1,9 @@
 // Fused SSP-RK stage kernel for n = 8 in the quad-fragment layout (sm_100a).
 //
 // Tile = (x element e, u element a, 4 consecutive v elements): 32 v-node columns, 8 x 8 (i, j)
-// rows.  Warp w owns v element w of the tile; inside a warp, lane = 4 g + t owns the two
-// output columns k = 2t, 2t + 1 of x node i = g, for all eight j.  That is the accumulator
+// rows.  Warps (w, h) own v element w of the tile and its j rows [h n / JS, (h + 1) n / JS)
+// (JS warps per element, 1 by default: two measured slower in FP64); inside a warp, lane = 4 g + t owns the two
+// output columns k = 2t, 2t + 1 of x node i = g, for the warp's j rows.  That is the accumulator
 // layout of the FP64 tensor-core instruction mma.m8n8k4 (D[g][2t..2t+1]), so per j the
 // x and v contractions run on the tensor cores (FP64 form) and land directly in the thread's
 // outputs:
@@ -22,11 +23,14 @@
 //   XF [side][j][32]     x upwind traces: (e-1, i = n-1) and (e+1, i = 0)
 //   UF [side][i][32]     u upwind traces: (a-1, j = n-1) and (a+1, j = 0)
 //   BG [table][j][32]    FP32 background split only: the eu and rb RHS tables of the tile
+//   UX [j]               u node coordinates of the tile's u element (bulk copy)
 // Two stages: tile q+1 streams in while tile q is computed.  Every wait is bounded: on timeout
 // the kernel raises bit 1 of the error word and returns.
 #pragma once
 
 #include <cuda.h>
+
+#include <type_traits>
 
 #include "vlasov_kernels.cuh"
 #include "vlasov_stage.cuh"
@@ -37,6 +41,13 @@
 #endif
 #ifndef VL_FRAG_MINB32
 #define VL_FRAG_MINB32 4
+#endif
+// warps per v element (each takes n / JS consecutive j rows)
+#ifndef VL_FRAG_JS64
+#define VL_FRAG_JS64 1
+#endif
+#ifndef VL_FRAG_JS32
+#define VL_FRAG_JS32 1
 #endif
 
 namespace vl {
@@ -52,7 +63,9 @@ struct FragGeom {
     static constexpr int PS = W * ROWS;              // IN plane stride: 324 | 360
     static constexpr int WF = COLS + P;              // FN row length: 34 | 36
     static constexpr int PSF = WF * ROWS;            // FN plane stride: 306 | 324
-    static constexpr int THREADS = 32 * EPT;
+    static constexpr int JS = sizeof(T) == 8 ? VL_FRAG_JS64 : VL_FRAG_JS32;   // warps per v element
+    static constexpr int NJ = N / JS;                // j rows per warp
+    static constexpr int THREADS = 32 * EPT * JS;
     static constexpr bool MMA = sizeof(T) == 8;      // tensor-core x/v contractions (FP64)
     static constexpr int MINB = sizeof(T) == 8 ? VL_FRAG_MINB64 : VL_FRAG_MINB32;   // CTAs per SM
     static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
@@ -63,7 +76,8 @@ struct FragGeom {
     // background-split RHS tables (a form of the FP32 context only)
     static constexpr bool BG = sizeof(T) == 4;
     static constexpr size_t BG_B = BG ? al(sizeof(float) * (size_t)2 * COLS * N) : 0;
-    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B;
+    static constexpr size_t UX_B = al(sizeof(double) * (size_t)N);
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
     static constexpr size_t smem_bytes() { return 2 * STAGE_B + 128; }
     static constexpr uint32_t TX_IN = sizeof(T) * W * ROWS * N;
     static constexpr uint32_t TX_FN = sizeof(T) * WF * ROWS * N;
@@ -113,11 +127,13 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     __shared__ __align__(8) uint64_t full[2];
-    __shared__ dd sRed[EPT][N];
+    __shared__ dd sRed[EPT * G::JS][N];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int w = tid >> 5;          // v element of the tile
+    const int wid = tid >> 5;
+    const int w = wid % EPT;         // v element of the tile
+    const int h = wid / EPT;         // j rows [h NJ, h NJ + NJ)
     const int g = lane >> 2;         // x node i of the thread's outputs
     const int t = lane & 3;          // columns 2t, 2t + 1 of the element
     const int wc = w * N;            // first tile column of the element
@@ -139,7 +155,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     const int kind = a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
     const bool with_bg = G::BG && a.bg_rb != nullptr;
-    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0);
+    const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0) +
+                              (uint32_t)sizeof(double) * N;
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile_cta = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -168,6 +185,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         tma_load_5d(uf, &maps.in_uface, &full[s], x0, N - 1, Ag - 1, 0, Eg);
         tma_load_5d(uf + sizeof(T) * COLS * N, &maps.in_uface, &full[s], x0, 0, Ag + 1, 0, Eg);
         if (with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
+        bulk_load(uf + G::UF_B + G::BG_B, a.u_nodes + Ag * N, (uint32_t)sizeof(double) * N, &full[s]);
         if (with_bg) {
             unsigned char *bg = uf + G::UF_B;
             tma_load_2d(bg, &maps.bg_eu, &full[s], x0, Ag * N);
@@ -230,10 +248,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const int Ag = au + 1;
         const bool act = w < nb;
         const int col = (b0 + 1) * N + cl;   // global v-node column of the first output
-        // node coordinates of the tile, read before the wait so their latency overlaps it
-        double uxs[N];
-#pragma unroll
-        for (int j = 0; j < N; ++j) uxs[j] = a.u_nodes[Ag * N + j];
+        // v-node coordinates of the thread's columns, read before the wait so their latency overlaps it
         const double vn0 = act ? a.v_nodes[col] : 0.0, vn1 = act ? a.v_nodes[col + 1] : 0.0;
         if (!mbar_wait_bounded(&full[s], (uint32_t)((q >> 1) & 1))) {
             if (a.err != nullptr) atomicOr(a.err, 2);
@@ -244,6 +259,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
         const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
         const float *sBG = reinterpret_cast<const float *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B);
+        const double *sUX =
+            reinterpret_cast<const double *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B + G::BG_B);
 
         if (act) {
             const double sd0 = accel * (Ei + bfield * vn0);
@@ -262,117 +279,131 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
             const size_t obase = (size_t)Eg * sE_ + (size_t)g * sI + (size_t)Ag * sA + col;
             T *pout = out + obase;
             const T *prow = sIn + g * PS + P + wc;   // row slice F[g][j][element] at j = 0
+            // the warp's j rows (compile-time j: table constants)
+            auto rows = [&](auto j0c) {
+                constexpr int J0 = decltype(j0c)::value;
 #pragma unroll
-            for (int j = 0; j < N; ++j) {
-                const double uxd = uxs[j];
-                const double svd = accel * (nbfield * uxd);
-                const bool xpos = uxd >= 0.0;
-                const bool vpos = svd >= 0.0;
-                T dx0, dx1, dv0, dv1;
-                if constexpr (G::MMA) {
-                    // x: A = upwind-folded up (rows g), B rows m = t, 4 + t at column wc + g, then
-                    // the neighbour trace of the thread's columns
-                    const T *pb = sIn + j * W + P + wc + g;
-                    const T b0v = pb[t * PS];
-                    const T b1v = pb[(4 + t) * PS];
-                    double x0 = 0.0, x1 = 0.0;
-                    dmma_8x8x4(x0, x1, xpos ? ca0 : ca0M, b0v);
-                    dmma_8x8x4(x0, x1, xpos ? ca1P : ca1, b1v);
-                    const V2 xn = *reinterpret_cast<const V2 *>(sXF + (xpos ? 0 : N * COLS) + j * COLS + cl);
-                    const T xcn = xpos ? xil : xir;
-                    dx0 = fma(xcn, xn.x, x0);
-                    dx1 = fma(xcn, xn.y, x1);
-                    // v: A = F[g][j][wc + 4c + t], B = upwind-folded up^T, then the neighbour
-                    // element's trace at row (g, j)
-                    const T *pa = prow + j * W;
-                    const T a0v = pa[t];
-                    const T a1v = pa[4 + t];
-                    double v0 = 0.0, v1 = 0.0;
-                    dmma_8x8x4(v0, v1, a0v, vpos ? ca0 : ca0M);
-                    dmma_8x8x4(v0, v1, a1v, vpos ? ca1P : ca1);
-                    const T vn = vpos ? pa[-1] : pa[N];
-                    dv0 = fma(vpos ? vil0 : vir0, vn, v0);
-                    dv1 = fma(vpos ? vil1 : vir1, vn, v1);
-                } else {
-                    const T *pc = sIn + j * W + P + cl;   // F[m][j][cl..cl+1] at m = 0
-                    dx0 = (T)0;
-                    dx1 = (T)0;
-                    V2 cm0, cm7;
-#pragma unroll
-                    for (int m = 0; m < N; ++m) {
-                        const V2 cv = *reinterpret_cast<const V2 *>(pc + m * PS);
-                        if (m == 0) cm0 = cv;
-                        if (m == N - 1) cm7 = cv;
-                        dx0 = fma(upi[m], cv.x, dx0);
-                        dx1 = fma(upi[m], cv.y, dx1);
+                for (int jj = 0; jj < G::NJ; ++jj) {
+                    const int j = J0 + jj;
+                    const double uxd = sUX[j];
+                    const double svd = accel * (nbfield * uxd);
+                    const bool xpos = uxd >= 0.0;
+                    const bool vpos = svd >= 0.0;
+                    T dx0, dx1, dv0, dv1;
+                    if constexpr (G::MMA) {
+                        // x: A = upwind-folded up (rows g), B rows m = t, 4 + t at column wc + g, then
+                        // the neighbour trace of the thread's columns
+                        const T *pb = sIn + j * W + P + wc + g;
+                        const T b0v = pb[t * PS];
+                        const T b1v = pb[(4 + t) * PS];
+                        double x0 = 0.0, x1 = 0.0;
+                        dmma_8x8x4(x0, x1, xpos ? ca0 : ca0M, b0v);
+                        dmma_8x8x4(x0, x1, xpos ? ca1P : ca1, b1v);
+                        const V2 xn = *reinterpret_cast<const V2 *>(sXF + (xpos ? 0 : N * COLS) + j * COLS + cl);
+                        const T xcn = xpos ? xil : xir;
+                        dx0 = fma(xcn, xn.x, x0);
+                        dx1 = fma(xcn, xn.y, x1);
+                        // v: A = F[g][j][wc + 4c + t], B = upwind-folded up^T, then the neighbour
+                        // element's trace at row (g, j)
+                        const T *pa = prow + j * W;
+                        const T a0v = pa[t];
+                        const T a1v = pa[4 + t];
+                        double v0 = 0.0, v1 = 0.0;
+                        dmma_8x8x4(v0, v1, a0v, vpos ? ca0 : ca0M);
+                        dmma_8x8x4(v0, v1, a1v, vpos ? ca1P : ca1);
+                        const T vn = vpos ? pa[-1] : pa[N];
+                        dv0 = fma(vpos ? vil0 : vir0, vn, v0);
+                        dv1 = fma(vpos ? vil1 : vir1, vn, v1);
+                    } else {
+                        const T *pc = sIn + j * W + P + cl;   // F[m][j][cl..cl+1] at m = 0
+                        dx0 = (T)0;
+                        dx1 = (T)0;
+                        V2 cm0, cm7;
+    #pragma unroll
+                        for (int m = 0; m < N; ++m) {
+                            const V2 cv = *reinterpret_cast<const V2 *>(pc + m * PS);
+                            if (m == 0) cm0 = cv;
+                            if (m == N - 1) cm7 = cv;
+                            dx0 = fma(upi[m], cv.x, dx0);
+                            dx1 = fma(upi[m], cv.y, dx1);
+                        }
+                        const V2 xf0 = *reinterpret_cast<const V2 *>(sXF + j * COLS + cl);
+                        const V2 xf1 = *reinterpret_cast<const V2 *>(sXF + N * COLS + j * COLS + cl);
+                        const V2 xl = xpos ? xf0 : cm0;
+                        const V2 xr = xpos ? cm7 : xf1;
+                        dx0 = fma(xig0, xl.x, dx0);
+                        dx0 = fma(-xig1, xr.x, dx0);
+                        dx1 = fma(xig0, xl.y, dx1);
+                        dx1 = fma(-xig1, xr.y, dx1);
+                        const T *pa = prow + j * W;
+                        T line[N];
+                        load_line<N, (sizeof(T) == 8 ? 2 : 4), T>(pa, line);
+                        dv0 = (T)0;
+                        dv1 = (T)0;
+    #pragma unroll
+                        for (int m = 0; m < N; ++m) {
+                            dv0 = fma(upk0[m], line[m], dv0);
+                            dv1 = fma(upk1[m], line[m], dv1);
+                        }
+                        const T tl = vpos ? pa[-1] : line[0];
+                        const T tr = vpos ? line[N - 1] : pa[N];
+                        dv0 = fma(xik00, tl, dv0);
+                        dv0 = fma(-xik01, tr, dv0);
+                        dv1 = fma(xik10, tl, dv1);
+                        dv1 = fma(-xik11, tr, dv1);
                     }
-                    const V2 xf0 = *reinterpret_cast<const V2 *>(sXF + j * COLS + cl);
-                    const V2 xf1 = *reinterpret_cast<const V2 *>(sXF + N * COLS + j * COLS + cl);
-                    const V2 xl = xpos ? xf0 : cm0;
-                    const V2 xr = xpos ? cm7 : xf1;
-                    dx0 = fma(xig0, xl.x, dx0);
-                    dx0 = fma(-xig1, xr.x, dx0);
-                    dx1 = fma(xig0, xl.y, dx1);
-                    dx1 = fma(-xig1, xr.y, dx1);
-                    const T *pa = prow + j * W;
-                    T line[N];
-                    load_line<N, (sizeof(T) == 8 ? 2 : 4), T>(pa, line);
-                    dv0 = (T)0;
-                    dv1 = (T)0;
-#pragma unroll
+                    // u: sum_m up[j][m] F[g][m][k] + lifts (compile-time j: table constants)
+                    T du0 = (T)0, du1 = (T)0;
+    #pragma unroll
                     for (int m = 0; m < N; ++m) {
-                        dv0 = fma(upk0[m], line[m], dv0);
-                        dv1 = fma(upk1[m], line[m], dv1);
+                        du0 = fma(tb.up[j * N + m], fu[m].x, du0);
+                        du1 = fma(tb.up[j * N + m], fu[m].y, du1);
                     }
-                    const T tl = vpos ? pa[-1] : line[0];
-                    const T tr = vpos ? line[N - 1] : pa[N];
-                    dv0 = fma(xik00, tl, dv0);
-                    dv0 = fma(-xik01, tr, dv0);
-                    dv1 = fma(xik10, tl, dv1);
-                    dv1 = fma(-xik11, tr, dv1);
+                    du0 = fma(tb.xi[2 * j], uL0, du0);
+                    du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
+                    du1 = fma(tb.xi[2 * j], uL1, du1);
+                    du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
+                    const T uxj = (T)uxd * jx, svj = (T)svd * jv;
+                    T r0 = fma(uxj, dx0, fma(spu0, du0, svj * dv0));
+                    T r1 = fma(uxj, dx1, fma(spu1, du1, svj * dv1));
+                    if (with_bg) {   // RHS of the x-independent background (staged with the tile)
+                        const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * COLS + cl);
+                        const float2 rb = *reinterpret_cast<const float2 *>(sBG + N * COLS + j * COLS + cl);
+                        r0 += (T)fmaf((float)Ei, eu.x, rb.x);
+                        r1 += (T)fmaf((float)Ei, eu.y, rb.y);
+                    }
+                    const V2 fij = *reinterpret_cast<const V2 *>(prow + j * W + 2 * t);
+                    V2 o;
+                    if (kind == KIND_RHS) {
+                        o.x = r0;
+                        o.y = r1;
+                    } else if (kind == KIND_EULER) {
+                        o.x = fma(dtT, r0, fij.x);
+                        o.y = fma(dtT, r1, fij.y);
+                    } else {
+                        const V2 fnv = *reinterpret_cast<const V2 *>(sFn + g * PSF + j * WF + P + cl);
+                        o.x = fma(c2dt, r0, fma(c1, fij.x, c0 * fnv.x));
+                        o.y = fma(c2dt, r1, fma(c1, fij.y, c0 * fnv.y));
+                    }
+                    *reinterpret_cast<V2 *>(pout + j * sJ) = o;
+                    if (gout != nullptr) {
+                        // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
+                        const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
+                        if (e == nx - 1) *reinterpret_cast<V2 *>(gout + gb) = fij;
+                        if (e == 0) *reinterpret_cast<V2 *>(gout + (size_t)(nx + 1) * sE_ + gb) = fij;
+                    }
+                    mk0 = fma(tb.wu[j], (double)o.x, mk0);
+                    mk1 = fma(tb.wu[j], (double)o.y, mk1);
                 }
-                // u: sum_m up[j][m] F[g][m][k] + lifts (compile-time j: table constants)
-                T du0 = (T)0, du1 = (T)0;
-#pragma unroll
-                for (int m = 0; m < N; ++m) {
-                    du0 = fma(tb.up[j * N + m], fu[m].x, du0);
-                    du1 = fma(tb.up[j * N + m], fu[m].y, du1);
-                }
-                du0 = fma(tb.xi[2 * j], uL0, du0);
-                du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
-                du1 = fma(tb.xi[2 * j], uL1, du1);
-                du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
-                const T uxj = (T)uxd * jx, svj = (T)svd * jv;
-                T r0 = fma(uxj, dx0, fma(spu0, du0, svj * dv0));
-                T r1 = fma(uxj, dx1, fma(spu1, du1, svj * dv1));
-                if (with_bg) {   // RHS of the x-independent background (staged with the tile)
-                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * COLS + cl);
-                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + N * COLS + j * COLS + cl);
-                    r0 += (T)fmaf((float)Ei, eu.x, rb.x);
-                    r1 += (T)fmaf((float)Ei, eu.y, rb.y);
-                }
-                const V2 fij = *reinterpret_cast<const V2 *>(prow + j * W + 2 * t);
-                V2 o;
-                if (kind == KIND_RHS) {
-                    o.x = r0;
-                    o.y = r1;
-                } else if (kind == KIND_EULER) {
-                    o.x = fma(dtT, r0, fij.x);
-                    o.y = fma(dtT, r1, fij.y);
-                } else {
-                    const V2 fnv = *reinterpret_cast<const V2 *>(sFn + g * PSF + j * WF + P + cl);
-                    o.x = fma(c2dt, r0, fma(c1, fij.x, c0 * fnv.x));
-                    o.y = fma(c2dt, r1, fma(c1, fij.y, c0 * fnv.y));
-                }
-                *reinterpret_cast<V2 *>(pout + j * sJ) = o;
-                if (gout != nullptr) {
-                    // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
-                    const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
-                    if (e == nx - 1) *reinterpret_cast<V2 *>(gout + gb) = fij;
-                    if (e == 0) *reinterpret_cast<V2 *>(gout + (size_t)(nx + 1) * sE_ + gb) = fij;
-                }
-                mk0 = fma(tb.wu[j], (double)o.x, mk0);
-                mk1 = fma(tb.wu[j], (double)o.y, mk1);
+            };
+            if constexpr (G::JS == 1) {
+                rows(std::integral_constant<int, 0>{});
+            } else {
+                static_assert(G::JS == 2, "one or two warps per v element");
+                if (h == 0)
+                    rows(std::integral_constant<int, 0>{});
+                else
+                    rows(std::integral_constant<int, G::NJ>{});
             }
         }
         __syncthreads();   // stage s fully consumed
@@ -384,12 +415,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     dd v = two_sum(tb.wv[2 * t] * mk0, tb.wv[2 * t + 1] * mk1);
     v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 1), __shfl_xor_sync(0xffffffffu, v.lo, 1)});
     v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 2), __shfl_xor_sync(0xffffffffu, v.lo, 2)});
-    if (t == 0) sRed[w][g] = v;
+    if (t == 0) sRed[wid][g] = v;
     __syncthreads();
     if (tid < N) {
         dd s = sRed[0][tid];
 #pragma unroll
-        for (int ww = 1; ww < EPT; ++ww) s = dd_add(s, sRed[ww][tid]);
+        for (int ww = 1; ww < EPT * G::JS; ++ww) s = dd_add(s, sRed[ww][tid]);
         a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * N + tid] = s.hi + s.lo;
     }
     (void)NT;
