@@ -68,6 +68,18 @@ struct StageArgs {
     const float *bg_eu;
 };
 
+// SSP-RK combination stage c0 f^n + c1 s + (c2 dt) r with c0 + c1 = 1 (main/timestep.py:157-163,
+// :174-182).  FP64 evaluates the reference's expression as written; FP32 evaluates
+// f^n + c1 (s - f^n) + (c2 dt) r, whose weights of f^n and s sum to exactly 1: with rounded
+// weights, float(1/3) + float(2/3) = 1 + 3e-8 would amplify every mode by 3e-8 per step.
+template <typename T>
+__device__ __forceinline__ T rk_combine(T c0, T c1, T c2dt, T fn, T s, T r) {
+    if constexpr (sizeof(T) == 4)
+        return fma(c2dt, r, fma(c1, s - fn, fn));
+    else
+        return fma(c2dt, r, fma(c1, s, c0 * fn));
+}
+
 // ----------------------------------------------------------------------------------------------
 // error-free transformation helpers for the FP64 moment reductions
 // ----------------------------------------------------------------------------------------------

@@ -290,7 +290,7 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
                 } else if (kind == KIND_EULER) {
                     o = fma(dtT, r, fij);
                 } else {
-                    o = fma(c2dt, r, fma(c1, fij, c0 * fn_cur[jc]));
+                    o = rk_combine(c0, c1, c2dt, fn_cur[jc], fij, r);
                 }
                 pout[i * sI + j * sJ] = o;
                 mrow = fma(wk[jc], (double)o, mrow);

@@ -419,8 +419,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     o.y = fma(dtT, r1, fij.y);
                 } else {
                     const V2 fnv = *reinterpret_cast<const V2 *>(sFn + i * PSF + j * WN + cs);
-                    o.x = fma(c2dt, r0, fma(c1, fij.x, c0 * fnv.x));
-                    o.y = fma(c2dt, r1, fma(c1, fij.y, c0 * fnv.y));
+                    o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
+                    o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
                 }
                 T *po = pout + (size_t)j * sJ;
                 if constexpr (N % 2 == 0) {

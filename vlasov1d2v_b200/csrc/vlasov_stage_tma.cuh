@@ -352,7 +352,7 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                         o = fma(dtT, r, fij);
                     } else {
                         const T fnv = G::STAGE_FN ? sFn[(i * N + j) * COLS + c] : pfn[i * sI + j * sJ];
-                        o = fma(c2dt, r, fma(c1, fij, c0 * fnv));
+                        o = rk_combine(c0, c1, c2dt, fnv, fij, r);
                     }
                     pout[i * sI + j * sJ] = o;
                     mrow = fma(wk[jc], (double)o, mrow);
