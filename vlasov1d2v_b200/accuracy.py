@@ -19,13 +19,14 @@ import numpy as np
 
 
 def run(res, order, steps, precision, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=0,
-        batch=64):
+        batch=64, background_split=True):
     import torch
 
     from . import problem
 
     p = problem.build(tuple(res), order, perturbation=perturbation, amp=amp, noise=noise,
-                      seed=seed, precision=precision, batch_steps=batch)
+                      seed=seed, precision=precision, batch_steps=batch,
+                      background_split=background_split)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, steps)
@@ -73,13 +74,17 @@ def main(argv=None):
     ap.add_argument("--perturbation", choices=("cos", "eigenmode"), default="cos",
                     help="cos: 1e-3 cos kx + 1e-6 noise; eigenmode: the reference's unstable "
                          "Bessel-series mode (om = -0.349i, delta_n = 1e-3)")
+    ap.add_argument("--no-split", action="store_true",
+                    help="FP32 run without the background split (plain FP32 state f)")
     args = ap.parse_args(argv)
     r64 = run(args.res, args.order, args.steps, "fp64", perturbation=args.perturbation)
-    r32 = run(args.res, args.order, args.steps, "fp32", perturbation=args.perturbation)
+    r32 = run(args.res, args.order, args.steps, "fp32", perturbation=args.perturbation,
+              background_split=not args.no_split)
     if args.save:
         np.savez(args.save, time64=r64["time"], energy64=r64["energy"], time32=r32["time"],
                  energy32=r32["energy"])
-    out = {"res": args.res, "order": args.order, "perturbation": args.perturbation}
+    out = {"res": args.res, "order": args.order, "perturbation": args.perturbation,
+           "fp32_background_split": not args.no_split}
     out.update(compare(r64, r32, tuple(args.window) if args.window else None))
     print(json.dumps(out))
     return 0
