@@ -24,6 +24,7 @@ struct vl_ctx {
     double xw[vl::NMAX];
     double qw[vl::NMAX * vl::NMAX];
     double *d_unodes = nullptr;
+    void *d_usv = nullptr;        // per u node (u, a (-B u)), double2 or float2
     double *d_vnodes = nullptr;
     double *d_k = nullptr;
     double *d_xw = nullptr;
@@ -36,6 +37,8 @@ struct vl_ctx {
     bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
     bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
     int stage_kernel = VL_STAGE_GEN;   // which stage kernel the launches use (vl_stage_kernel)
+    bool use_pdl = false;         // loop launches with programmatic dependent launch
+    bool pdl_now = false;         // set while vl_ssp_rk3_steps issues its launches
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
     const float *bg_eu = nullptr;
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer

@@ -51,6 +51,8 @@ struct StageArgs {
     const double *dt;      // device scalar
     const vl_run_state *state;  // when not null, the kernel returns if !state->active
     const double *u_nodes; // [(nu+2) n]
+    const void *usv;       // [(nu+2) n] pairs (u, a (-B u)) in the state precision: the x and v
+                           // flux speeds per u node (n = 8 kernel)
     const double *v_nodes; // [(nv+2) n]
     double *partials;      // [nx][G][n] moment partials of out, or null
     const double *tables;  // device copy: up [n n], xi [n 2], qw [n n] (per-lane indexed reads)
@@ -67,6 +69,16 @@ struct StageArgs {
     const float *bg_rb;
     const float *bg_eu;
 };
+
+// Programmatic dependent launch (opt-in, VLASOV1D2V_PDL=1).  Inside the RK loop every kernel is
+// then launched so that it may
+// start while its predecessor on the stream finishes; before reading anything the predecessor
+// writes it waits for that grid's completion (a no-op for a plain launch), and only then lets its
+// own dependents launch.  Every kernel waits before any exit, so the completion of a kernel
+// implies the completion of all earlier ones, and a kernel that has started may read data
+// written two or more launches back (loop state, the previous stage's output).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // SSP-RK combination stage c0 f^n + c1 s + (c2 dt) r with c0 + c1 = 1 (main/timestep.py:157-163,
 // :174-182).  FP64 evaluates the reference's expression as written; FP32 evaluates
@@ -151,6 +163,7 @@ constexpr int MOMENT_CTAS_PER_SM = 4;
 
 template <int N, typename T>
 __global__ void __launch_bounds__(MOMENT_THREADS, MOMENT_CTAS_PER_SM) moment_kernel(const MomentArgs a) {
+    pdl_wait();
     const T *__restrict__ f = static_cast<const T *>(a.f);
     constexpr int CT = (MOMENT_THREADS / N) * N;   // column threads (stride keeps k fixed)
     const int g = blockIdx.x, Gn = gridDim.x, e = blockIdx.y;
@@ -356,6 +369,8 @@ __device__ __forceinline__ void field_fwd_body(const FieldArgs &a, int bx) {
 }
 
 static __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArgs a) {
+    pdl_wait();
+    pdl_trigger();
     field_fwd_body(a, blockIdx.x);
 }
 
@@ -467,6 +482,8 @@ __device__ __forceinline__ void field_inv_body(const FieldArgs &a, int bx, int n
 }
 
 static __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArgs a) {
+    pdl_wait();
+    pdl_trigger();
     field_inv_body(a, blockIdx.x, gridDim.x);
 }
 

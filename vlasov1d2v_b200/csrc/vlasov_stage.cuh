@@ -334,6 +334,8 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
 template <int N, typename T>
 __global__ void __launch_bounds__(PencilGeom<N, T>::THREADS, PencilGeom<N, T>::MIN_BLOCKS)
 stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
+    pdl_wait();
+    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
     pencil_stage_body<N, T, PencilGeom<N, T>::JC, PencilGeom<N, T>::THREADS>(
         a, tb, tb.qw, blockIdx.y, blockIdx.x, gridDim.x);

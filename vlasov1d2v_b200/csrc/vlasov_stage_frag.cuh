@@ -23,7 +23,7 @@
 //   XF [side][j][32]     x upwind traces: (e-1, i = n-1) and (e+1, i = 0)
 //   UF [side][i][32]     u upwind traces: (a-1, j = n-1) and (a+1, j = 0)
 //   BG [table][j][32]    FP32 background split only: the eu and rb RHS tables of the tile
-//   UX [j]               u node coordinates of the tile's u element (bulk copy)
+//   US [j]               the x and v flux speeds (u, a (-B u)) of the tile's u nodes (bulk copy)
 // Two stages: tile q+1 streams in while tile q is computed.  Every wait is bounded: on timeout
 // the kernel raises bit 1 of the error word and returns.
 #pragma once
@@ -82,7 +82,7 @@ struct FragGeom {
     // background-split RHS tables (a form of the FP32 context only)
     static constexpr bool BG = sizeof(T) == 4;
     static constexpr size_t BG_B = BG ? al(sizeof(float) * (size_t)2 * COLS * N) : 0;
-    static constexpr size_t UX_B = al(sizeof(double) * (size_t)N);
+    static constexpr size_t UX_B = al(2 * sizeof(T) * (size_t)N);
     static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
     static constexpr size_t smem_bytes() { return 2 * STAGE_B + 128; }
     static constexpr uint32_t TX_IN = sizeof(T) * W * ROWS * N;
@@ -156,7 +156,11 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     using V2 = typename Pair<T>::V;
     constexpr int N = G::N, P = G::P, W = G::W, PS = G::PS, WF = G::WF, PSF = G::PSF;
     constexpr int COLS = G::COLS, EPT = G::EPT, NT = G::THREADS;
-    if (a.state != nullptr && a.state->active == 0) return;
+    // loop state written two or more launches back: readable before the dependency wait
+    if (a.state != nullptr && a.state->active == 0) {
+        pdl_wait();
+        return;
+    }
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
@@ -191,7 +195,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     const bool with_fn = (kind == KIND_COMBINE);
     const bool with_bg = G::BG && a.bg_rb != nullptr;
     const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0) +
-                              (uint32_t)sizeof(double) * N;
+                              (uint32_t)(2 * sizeof(T)) * N;
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile_cta = (blockIdx.x < tiles) ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
@@ -220,7 +224,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         tma_load_5d(uf, &maps.in_uface, &full[s], x0, N - 1, Ag - 1, 0, Eg);
         tma_load_5d(uf + sizeof(T) * COLS * N, &maps.in_uface, &full[s], x0, 0, Ag + 1, 0, Eg);
         if (with_fn) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
-        bulk_load(uf + G::UF_B + G::BG_B, a.u_nodes + Ag * N, (uint32_t)sizeof(double) * N, &full[s]);
+        bulk_load(uf + G::UF_B + G::BG_B, static_cast<const V2 *>(a.usv) + Ag * N, (uint32_t)(2 * sizeof(T)) * N,
+                  &full[s]);
         if (with_bg) {
             unsigned char *bg = uf + G::UF_B;
             tma_load_2d(bg, &maps.bg_eu, &full[s], x0, Ag * N);
@@ -231,8 +236,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         if (ntile_cta > 0) issue(0, 0);
         if (ntile_cta > 1) issue(1, 1);
     }
+    // the first tiles (the previous stage's output) stream in while the field solve finishes;
+    // E comes from the immediately preceding launch
+    pdl_wait();
+    pdl_trigger();
 
-    const double accel = a.accel, bfield = a.bfield, nbfield = -a.bfield;
+    const double accel = a.accel, bfield = a.bfield;
     const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
     const T dtT = (T)dtd, c0 = (T)a.c0, c1 = (T)a.c1, c2dt = (T)(a.c2 * dtd);
     const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
@@ -307,8 +316,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         const T *sXF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B);
         const T *sUF = reinterpret_cast<const T *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B);
         const float *sBG = reinterpret_cast<const float *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B);
-        const double *sUX =
-            reinterpret_cast<const double *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B + G::BG_B);
+        const V2 *sUS =
+            reinterpret_cast<const V2 *>(stage_ptr(s) + G::IN_B + G::FN_B + G::XF_B + G::UF_B + G::BG_B);
 
         if (act) {
             const double sd0 = accel * (Ei + bfield * vn0);
@@ -333,10 +342,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
 #pragma unroll
                 for (int jj = 0; jj < G::NJ; ++jj) {
                     const int j = J0 + jj;
-                    const double uxd = sUX[j];
-                    const double svd = accel * (nbfield * uxd);
-                    const bool xpos = uxd >= 0.0;
-                    const bool vpos = svd >= 0.0;
+                    // x and v flux speeds (their signs are the upwind directions) times the
+                    // direction weights
+                    const V2 us = sUS[j];
+                    const bool xpos = us.x >= (T)0;
+                    const bool vpos = us.y >= (T)0;
+                    const T uxj = us.x * jx, svj = us.y * jv;
                     T dx0, dx1, dv0, dv1;
                     if constexpr (G::MMA) {
                         // x: A = upwind-folded up (rows g), B rows m = t, 4 + t at column wc + g, then
@@ -439,7 +450,6 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
                     du1 = fma(tb.xi[2 * j], uL1, du1);
                     du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
-                    const T uxj = (T)uxd * jx, svj = (T)svd * jv;
                     T r0 = fma(uxj, dx0, fma(spu0, du0, svj * dv0));
                     T r1 = fma(uxj, dx1, fma(spu1, du1, svj * dv1));
                     if (with_bg) {   // RHS of the x-independent background (staged with the tile)

@@ -467,6 +467,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
 template <int N, typename T>
 __global__ void __launch_bounds__(GenGeom<N, T>::THREADS, GenGeom<N, T>::MINB)
 stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
+    pdl_wait();
+    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
