@@ -172,6 +172,43 @@ int bg_map(vl_ctx *c, const float *ptr, int n, CUtensorMap *out) {
     return VL_OK;
 }
 
+// 5-D view of an FP64 state for the generic kernel's TMA form: which 0 = tile (WB, RJ, 1, n, 1),
+// 1 = x-node plane (WB, n, 1, 1, 1), 2 = j row of every x node (WB, 1, 1, n, 1)
+template <int N>
+int gen_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
+    using G = vl::GenTmaGeom<N, double>;
+    auto key = std::make_pair(ptr, 20 + which);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2, X = c->cfg.nx + 2, es = sizeof(double);
+    cuuint64_t dims[5] = {V * N, (cuuint64_t)N, U, (cuuint64_t)N, X};
+    cuuint64_t strides[4] = {V * N * es, V * N * N * es, V * N * N * U * es, V * N * N * U * N * es};
+    cuuint32_t box[5] = {(cuuint32_t)G::WB, 1, 1, 1, 1};
+    if (which == 0) {
+        box[1] = G::RJ;
+        box[3] = N;
+    } else if (which == 1) {
+        box[1] = N;
+    } else {
+        box[3] = N;
+    }
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (generic kernel) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
 template <int N, typename T>
 int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageTables<T> tb;
@@ -213,6 +250,23 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             return check_launch(launch(c, vl::stage_frag_kernel<T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a, tb,
                                        maps),
                                 "stage_frag_kernel");
+        }
+    }
+    if constexpr (sizeof(T) == 8) {
+        if (c->stage_kernel == VL_STAGE_GEN && c->gen_tma) {
+            using G = vl::GenTmaGeom<N, double>;
+            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out)) % 16)
+                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
+            vl::GenMaps maps;
+            int rc;
+            if ((rc = gen_map<N>(c, a.in, 0, &maps.in_tile))) return rc;
+            if ((rc = gen_map<N>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
+            if ((rc = gen_map<N>(c, a.in, 1, &maps.xface))) return rc;
+            if ((rc = gen_map<N>(c, a.in, 2, &maps.uface))) return rc;
+            return check_launch(launch(c, vl::stage_gen_tma_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s,
+                                       a, tb, maps),
+                                "stage_gen_tma_kernel");
         }
     }
     if (c->stage_kernel == VL_STAGE_GEN) {
@@ -267,8 +321,19 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag, bool gen) {
+int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
     int blocks = 0;
+    if constexpr (sizeof(T) == 8) {
+        if (gen && gtma) {
+            using G = vl::GenTmaGeom<N, double>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_gen_tma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_tma_kernel<N>, G::THREADS,
+                                                              smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
+    }
     if (gen) {
         using G = vl::GenGeom<N, T>;
         const size_t smem = G::smem_bytes();
@@ -321,18 +386,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag, bool gen) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag, gen);
-        case 2: return stage_occupancy_t<2, T>(tma, frag, gen);
-        case 3: return stage_occupancy_t<3, T>(tma, frag, gen);
-        case 4: return stage_occupancy_t<4, T>(tma, frag, gen);
-        case 5: return stage_occupancy_t<5, T>(tma, frag, gen);
-        case 6: return stage_occupancy_t<6, T>(tma, frag, gen);
-        case 7: return stage_occupancy_t<7, T>(tma, frag, gen);
-        case 8: return stage_occupancy_t<8, T>(tma, frag, gen);
-        case 9: return stage_occupancy_t<9, T>(tma, frag, gen);
-        case 10: return stage_occupancy_t<10, T>(tma, frag, gen);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma);
         default: return 1;
     }
 }
@@ -660,8 +725,15 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         if (c->stage_kernel != VL_STAGE_TMA && c->stage_kernel != VL_STAGE_FRAG) c->use_tma = false;
     }
     const bool gen = c->stage_kernel == VL_STAGE_GEN;
-    const int occ = cfg->precision == VL_FP64 ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen)
-                                              : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen);
+    // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even)
+    {
+        const char *env = getenv("VLASOV1D2V_GEN_NO_TMA");
+        c->gen_tma = gen && cfg->precision == VL_FP64 && ((size_t)(cfg->nv + 2) * n) % 2 == 0 &&
+                     encode_fn() != nullptr && !(env && env[0] == '1');
+    }
+    const int occ = cfg->precision == VL_FP64
+                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma)
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, false);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double

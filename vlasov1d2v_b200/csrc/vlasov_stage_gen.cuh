@@ -26,11 +26,22 @@
 //   UX [j]            u node coordinates of the tile's u element
 // W and WN are padded so that the k-line loads of the up-to-eight x nodes met by one warp fall
 // in distinct banks (searched at compile time for the actual lane assignment).
+//
+// TMA form (FP64 with 16-byte-aligned state rows, stage_gen_tma_kernel): one thread per CTA loads
+// each array of the tile with one cp.async.bulk.tensor box (no multicast) into the same stages,
+// completing on an mbarrier (bounded waits).  Rows are then contiguous copies of the state: the
+// tile starts at the 16-byte boundary at or below the left v trace, element b's node k sits at
+// column off + 1 + b n + k (off = 0 or 1 per tile), and the column pairs are read as two scalar
+// loads.  Every box lands on a 128-byte-aligned shared-memory address.  Row lengths hold an odd number of 16-byte units and planes an odd number of rows, so
+// the loads of eight x nodes at one column fall in distinct banks.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "vlasov_kernels.cuh"
+#include "vlasov_stage_tma.cuh"
 
 namespace vl {
 
@@ -143,6 +154,68 @@ struct GenGeom {
     static_assert(ITEMS <= THREADS, "items exceed threads");
 };
 
+// tensor maps of the TMA form (5-D views of the state: v node, j, a, i, e)
+struct GenMaps {
+    CUtensorMap in_tile;   // box (WB, RJ, 1, n, 1) over the stage input
+    CUtensorMap fn_tile;   // the same box over f^n
+    CUtensorMap xface;     // box (WB, n, 1, 1, 1): one x node plane
+    CUtensorMap uface;     // box (WB, 1, 1, n, 1): one j row of every x node
+};
+
+template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
+struct GenTmaGeom {
+    static_assert(sizeof(T) == 8, "the TMA form serves FP64 states");
+    static constexpr int EPT = EPT_;
+    static constexpr int Q = 16 / (int)sizeof(T);                       // elements per 16 bytes
+    static constexpr int WB0 = (EPT * N + 2 + 2 * (Q - 1)) / Q * Q;     // tile + both traces, any offset
+    static constexpr int WB = ((WB0 / Q) % 2 == 1) ? WB0 : WB0 + Q;    // odd number of 16-byte units
+    static constexpr int RJ = N + ((N % 2 == 0) ? 1 : 0);              // j rows per plane (odd)
+    static constexpr int PS = RJ * WB;                                  // plane stride
+    static constexpr int UXC = N + (N & 1);                             // u nodes copied from an even start
+    static constexpr int THREADS = GenGeom<N, T, EPT>::THREADS;
+    static constexpr int NST = 2;
+    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
+    static constexpr size_t IN_B = al(sizeof(T) * (size_t)N * PS);
+    static constexpr size_t FN_B = IN_B;
+    // each face side starts on a 128-byte boundary (tensor copies into shared memory need it)
+    static constexpr size_t FSIDE_B = al(sizeof(T) * (size_t)N * WB);
+    static constexpr size_t XF_B = 2 * FSIDE_B;
+    static constexpr size_t UF_B = XF_B;
+    static constexpr size_t UX_B = al(sizeof(double) * (size_t)UXC);
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + UX_B;
+    static constexpr uint32_t TX_IN = sizeof(T) * WB * RJ * N;
+    static constexpr uint32_t TX_FACE = sizeof(T) * WB * N;
+    static constexpr uint32_t TX_UX = sizeof(double) * UXC;
+    static constexpr size_t smem_bytes() {
+        const size_t s = NST * STAGE_B;
+        const size_t red = sizeof(dd) * (size_t)THREADS;
+        return (s > red ? s : red) + 128;
+    }
+    static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
+    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * 168);
+    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
+    static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
+    static_assert(WB <= 256, "TMA box width");
+};
+
+// shared-memory layout constants of the two forms (row lengths, plane strides, array bytes)
+template <bool TMA, int N, typename T, int EPT>
+struct GenLayout {
+    using GG = GenGeom<N, T, EPT>;
+    static constexpr int RIN = GG::W, PIN = GG::PS, RFN = GG::WN, PFN = GG::PSF, RFC = GG::WF, Q = 1;
+    static constexpr int FS = N * GG::WF;   // offset of the second face side (elements)
+    static constexpr size_t S_IN = GG::IN_B, S_FN = GG::FN_B, S_XF = GG::XF_B, S_UF = GG::UF_B;
+    static constexpr size_t S_BG = GG::BG_B, S_STAGE = GG::STAGE_B;
+};
+template <int N, typename T, int EPT>
+struct GenLayout<true, N, T, EPT> {
+    using GT = GenTmaGeom<N, T, EPT>;
+    static constexpr int RIN = GT::WB, PIN = GT::PS, RFN = GT::WB, PFN = GT::PS, RFC = GT::WB, Q = GT::Q;
+    static constexpr int FS = (int)(GT::FSIDE_B / sizeof(T));
+    static constexpr size_t S_IN = GT::IN_B, S_FN = GT::FN_B, S_XF = GT::XF_B, S_UF = GT::UF_B;
+    static constexpr size_t S_BG = 0, S_STAGE = GT::STAGE_B;
+};
+
 template <typename T>
 struct GenPair;
 template <>
@@ -158,13 +231,25 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB>
+template <int N, typename T, int EPT, typename TB, bool TMA = false>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
-                                               int g, int G, unsigned char *smem) {
+                                               int g, int G, unsigned char *smem,
+                                               const GenMaps *maps = nullptr) {
     using GG = GenGeom<N, T, EPT>;
     using V2 = typename GenPair<T>::V;
     constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
     constexpr int PS = GG::PS, PSF = GG::PSF, NST = GG::NST, NW = GG::NW, NT = GG::THREADS;
+    // shared-memory geometry of the form in use (TMA: contiguous rows of the state)
+    using L = GenLayout<TMA, N, T, EPT>;
+    constexpr int RIN = L::RIN;      // IN row length
+    constexpr int PIN = L::PIN;      // IN plane stride
+    constexpr int RFN = L::RFN;      // FN row length
+    constexpr int PFN = L::PFN;      // FN plane stride
+    constexpr int RFC = L::RFC;      // face / background row length
+    constexpr size_t S_IN = L::S_IN, S_FN = L::S_FN, S_XF = L::S_XF, S_UF = L::S_UF;
+    constexpr size_t S_BG = L::S_BG, S_STAGE = L::S_STAGE;
+    constexpr int FS = L::FS;        // second face side (elements)
+    __shared__ __align__(8) uint64_t gfull[2];   // TMA form: one mbarrier per stage
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -208,12 +293,20 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     // (computed, not stored) stay finite
     {
         uint4 *z = reinterpret_cast<uint4 *>(smem);
-        const int nz = (int)(NST * GG::STAGE_B / 16);
+        const int nz = (int)(NST * S_STAGE / 16);
         for (int q = tid; q < nz; q += blockDim.x) z[q] = make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
 
-    auto stage_ptr = [&](int s) { return smem + (size_t)s * GG::STAGE_B; };
+    if constexpr (TMA) {
+        if (tid == 0) {
+            mbar_init(&gfull[0], 1);
+            mbar_init(&gfull[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
+    auto stage_ptr = [&](int s) { return smem + (size_t)s * S_STAGE; };
     // one row of ncol tile columns: global run -> slot layout
     auto copy_row = [&](T *dst, const T *src, int ncol) {
         if constexpr (N % 2 == 0) {
@@ -283,6 +376,31 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         }
         if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
     };
+    // TMA form: one thread loads the tile's boxes into stage s
+    auto issue_tma = [&](int s, int tt) {
+        if constexpr (TMA) {
+            using GT = GenTmaGeom<N, T, EPT>;
+            const int au = tt / nbt;
+            const int b0 = (tt - au * nbt) * EPT;
+            const int Ag = au + 1;
+            const int xs = ((b0 + 1) * N - 1) & ~(GT::Q - 1);
+            unsigned char *st = stage_ptr(s);
+            unsigned char *xf = st + S_IN + S_FN;
+            unsigned char *uf = xf + S_XF;
+            const uint32_t tx = GT::TX_IN * (with_fn ? 2 : 1) + 4 * GT::TX_FACE + GT::TX_UX;
+            mbar_arrive_expect_tx(&gfull[s], tx);
+            tma_load_5d(st, &maps->in_tile, &gfull[s], xs, 0, Ag, 0, Eg);
+            if (with_fn) tma_load_5d(st + S_IN, &maps->fn_tile, &gfull[s], xs, 0, Ag, 0, Eg);
+            tma_load_5d(xf, &maps->xface, &gfull[s], xs, 0, Ag, N - 1, El);
+            tma_load_5d(xf + GT::FSIDE_B, &maps->xface, &gfull[s], xs, 0, Ag, 0, Er);
+            tma_load_5d(uf, &maps->uface, &gfull[s], xs, N - 1, Ag - 1, 0, Eg);
+            tma_load_5d(uf + GT::FSIDE_B, &maps->uface, &gfull[s], xs, 0, Ag + 1, 0, Eg);
+            bulk_load(uf + S_UF, a.u_nodes + ((Ag * N) & ~1), GT::TX_UX, &gfull[s]);
+        } else {
+            (void)s;
+            (void)tt;
+        }
+    };
 
     const double accel = a.accel, bfield = a.bfield, nbfield = -a.bfield;
     const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
@@ -302,15 +420,24 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     const double wf0 = wfin[k0], wf1 = pad1 ? 0.0 : wfin[k1];
     double mk0 = 0.0, mk1 = 0.0;   // sum_j wu_j out[.., j, k] for the two columns
 
+    if constexpr (TMA) {
+        if (tid == 0) {
+            if (ntile > 0) issue_tma(0, g);
+            if (ntile > 1) issue_tma(1, g + G);
+        }
+    } else {
 #pragma unroll
-    for (int s0 = 0; s0 < NST - 1; ++s0) {
-        if (s0 < ntile) issue(s0, g + s0 * G);
-        cp_async_commit();
+        for (int s0 = 0; s0 < NST - 1; ++s0) {
+            if (s0 < ntile) issue(s0, g + s0 * G);
+            cp_async_commit();
+        }
     }
     for (int q = 0; q < ntile; ++q) {
-        const int qn = q + NST - 1;
-        if (qn < ntile) issue(qn % NST, g + qn * G);
-        cp_async_commit();
+        if constexpr (!TMA) {
+            const int qn = q + NST - 1;
+            if (qn < ntile) issue(qn % NST, g + qn * G);
+            cp_async_commit();
+        }
         const int tt = g + q * G;
         const int au = tt / nbt;
         const int b0 = (tt - au * nbt) * EPT;
@@ -319,29 +446,52 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         const bool act = has_item && b < nb;
         const int col = (b0 + b + 1) * N + 2 * p;    // global v-node column of the pair
         const double vn0 = act ? a.v_nodes[col] : 0.0, vn1 = act ? a.v_nodes[col + 1] : 0.0;
-        cp_async_wait<NST - 1>();
-        __syncthreads();   // tile q visible to every thread
+        if constexpr (TMA) {
+            if (!mbar_wait_bounded(&gfull[q & 1], (uint32_t)((q >> 1) & 1))) {
+                if (a.err != nullptr) atomicOr(a.err, 2);
+                return;
+            }
+        } else {
+            cp_async_wait<NST - 1>();
+            __syncthreads();   // tile q visible to every thread
+        }
         const unsigned char *st = stage_ptr(q % NST);
         const T *sIn = reinterpret_cast<const T *>(st);
-        const T *sFn = reinterpret_cast<const T *>(st + GG::IN_B);
-        const T *sXF = reinterpret_cast<const T *>(st + GG::IN_B + GG::FN_B);
-        const T *sUF = reinterpret_cast<const T *>(st + GG::IN_B + GG::FN_B + GG::XF_B);
-        const float *sBG = reinterpret_cast<const float *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B);
-        const double *sUX =
-            reinterpret_cast<const double *>(st + GG::IN_B + GG::FN_B + GG::XF_B + GG::UF_B + GG::BG_B);
+        const T *sFn = reinterpret_cast<const T *>(st + S_IN);
+        const T *sXF = reinterpret_cast<const T *>(st + S_IN + S_FN);
+        const T *sUF = reinterpret_cast<const T *>(st + S_IN + S_FN + S_XF);
+        const float *sBG = reinterpret_cast<const float *>(st + S_IN + S_FN + S_XF + S_UF);
+        const double *sUX0 = reinterpret_cast<const double *>(st + S_IN + S_FN + S_XF + S_UF + S_BG);
+        // column of element b's node 0 in the IN rows, of the thread's pair in IN and in the
+        // FN / face / background rows; first u node in sUX
+        const int cL = (b0 + 1) * N - 1;
+        const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : H + b * SL;
+        const int cin = ebase + 2 * p;
+        const int cfc = TMA ? cin : cs;
+        const double *sUX = sUX0 + (TMA ? ((Ag * N) & 1) : 0);
+        auto ld2 = [&](const T *q2) -> V2 {
+            if constexpr (TMA) {
+                V2 r;
+                r.x = q2[0];
+                r.y = q2[1];
+                return r;
+            } else {
+                return *reinterpret_cast<const V2 *>(q2);
+            }
+        };
         if (act) {
             const double sd0 = accel * (Ei + bfield * vn0);
             const double sd1 = accel * (Ei + bfield * vn1);
             const T sp0 = (T)sd0, sp1 = (T)sd1;
             V2 fu[N];
 #pragma unroll
-            for (int m = 0; m < N; ++m) fu[m] = *reinterpret_cast<const V2 *>(sIn + i * PS + m * W + H + cs);
-            const V2 ufl = *reinterpret_cast<const V2 *>(sUF + i * WF + cs);
-            const V2 ufr = *reinterpret_cast<const V2 *>(sUF + (N + i) * WF + cs);
+            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin);
+            const V2 ufl = ld2(sUF + i * RFC + cfc);
+            const V2 ufr = ld2(sUF + FS + i * RFC + cfc);
             const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
             const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
             T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
-            const T *prow = sIn + i * PS + H + b * SL;   // k-line of element b at j = 0
+            const T *prow = sIn + i * PIN + ebase;   // k-line of element b at j = 0
 #pragma unroll
             for (int j = 0; j < N; ++j) {
                 const double uxd = sUX[j];
@@ -349,19 +499,19 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 const bool xpos = uxd >= 0.0;
                 const bool vpos = svd >= 0.0;
                 // x: sum_m up[i][m] F[m][j][k] + lifts
-                const T *pc = sIn + j * W + H + cs;
+                const T *pc = sIn + j * RIN + cin;
                 T dx0 = (T)0, dx1 = (T)0;
                 V2 cm0, cmL;
 #pragma unroll
                 for (int m = 0; m < N; ++m) {
-                    const V2 cv = *reinterpret_cast<const V2 *>(pc + m * PS);
+                    const V2 cv = ld2(pc + m * PIN);
                     if (m == 0) cm0 = cv;
                     if (m == N - 1) cmL = cv;
                     dx0 = fma(upi[m], cv.x, dx0);
                     dx1 = fma(upi[m], cv.y, dx1);
                 }
-                const V2 xf0 = *reinterpret_cast<const V2 *>(sXF + j * WF + cs);
-                const V2 xf1 = *reinterpret_cast<const V2 *>(sXF + (N + j) * WF + cs);
+                const V2 xf0 = ld2(sXF + j * RFC + cfc);
+                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc);
                 const V2 xl = xpos ? xf0 : cm0;
                 const V2 xr = xpos ? cmL : xf1;
                 dx0 = fma(xig0, xl.x, dx0);
@@ -369,11 +519,11 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 dx1 = fma(xig0, xl.y, dx1);
                 dx1 = fma(-xig1, xr.y, dx1);
                 // v: sum_m F[i][j][m] up[k][m] + lifts (the element's k-line)
-                const T *pa = prow + j * W;
+                const T *pa = prow + j * RIN;
                 T line[2 * P];
 #pragma unroll
                 for (int m2 = 0; m2 < P; ++m2) {
-                    const V2 l2 = *reinterpret_cast<const V2 *>(pa + 2 * m2);
+                    const V2 l2 = ld2(pa + 2 * m2);
                     line[2 * m2] = l2.x;
                     line[2 * m2 + 1] = l2.y;
                 }
@@ -383,8 +533,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     dv0 = fma(upk0[m], line[m], dv0);
                     dv1 = fma(upk1[m], line[m], dv1);
                 }
-                const T tl = vpos ? pa[LH - H] : line[0];
-                const T tr = vpos ? line[N - 1] : pa[SL];
+                const T tl = vpos ? pa[TMA ? -1 : LH - H] : line[0];
+                const T tr = vpos ? line[N - 1] : pa[TMA ? N : SL];
                 dv0 = fma(xik00, tl, dv0);
                 dv0 = fma(-xik01, tr, dv0);
                 dv1 = fma(xik10, tl, dv1);
@@ -404,8 +554,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
                 T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
                 if (with_bg) {   // RHS of the x-independent background
-                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * WF + cs);
-                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + (N + j) * WF + cs);
+                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * RFC + cfc);
+                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + N * RFC + j * RFC + cfc);
                     r0 += (T)fmaf((float)Ei, eu.x, rb.x);
                     r1 += (T)fmaf((float)Ei, eu.y, rb.y);
                 }
@@ -418,7 +568,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     o.x = fma(dtT, r0, fij.x);
                     o.y = fma(dtT, r1, fij.y);
                 } else {
-                    const V2 fnv = *reinterpret_cast<const V2 *>(sFn + i * PSF + j * WN + cs);
+                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc);
                     o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
                     o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
                 }
@@ -446,6 +596,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             }
         }
         __syncthreads();   // stage q % NST consumed before it is refilled
+        if constexpr (TMA) {
+            if (tid == 0 && q + 2 < ntile) issue_tma(q & 1, g + (q + 2) * G);
+        }
     }
     cp_async_wait<0>();
 
@@ -474,6 +627,21 @@ stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
     gen_stage_body<N, T, GenGeom<N, T>::EPT>(a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
+}
+
+// TMA form (FP64, 16-byte-aligned state rows)
+template <int N>
+__global__ void __launch_bounds__(GenTmaGeom<N, double>::THREADS, GenTmaGeom<N, double>::MINB)
+stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<double> tb,
+                     const __grid_constant__ GenMaps maps) {
+    pdl_wait();
+    pdl_trigger();
+    if (a.state != nullptr && a.state->active == 0) return;
+    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
+    gen_stage_body<N, double, GenGeom<N, double>::EPT, StageTables<double>, true>(
+        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
 }
 
 }  // namespace vl

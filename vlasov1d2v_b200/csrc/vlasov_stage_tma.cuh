@@ -24,6 +24,7 @@
 #include <type_traits>
 
 #include "vlasov_kernels.cuh"
+#include "vlasov_stage.cuh"
 
 #ifndef VL_TMA_JC64
 #define VL_TMA_JC64 2
