@@ -699,19 +699,14 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         const char *env = getenv("VLASOV1D2V_NO_FRAG");
         if (env && env[0] == '1') c->use_frag = false;
     }
-    // stage kernel (fastest measured per order and precision): the fragment kernel for n = 8, the
-    // TMA kernel for the other aligned orders (n = 2, 4), then the asynchronous-copy kernel in FP64
-    // and the register-pencil kernel in FP32; VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects
-    // one for comparisons
-    {
-        // programmatic dependent launch in the loop: measured 0.4% (FP64) to 2.6% (FP32) slower
-        // per step on B200, so off unless VLASOV1D2V_PDL=1
-        const char *env = getenv("VLASOV1D2V_PDL");
-        c->use_pdl = env && env[0] == '1';
-    }
-    c->stage_kernel = c->use_frag ? VL_STAGE_FRAG
-                    : c->use_tma  ? VL_STAGE_TMA
-                    : (cfg->precision == VL_FP64 ? VL_STAGE_GEN : VL_STAGE_PENCIL);
+    // stage kernel (fastest measured per order and precision): the fragment kernel for n = 8; in
+    // FP64 the generic kernel for every other order (its TMA form where the rows allow); in FP32
+    // the TMA kernel for n = 4 and the register-pencil kernel otherwise.
+    // VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects one for comparisons
+    c->stage_kernel = c->use_frag                    ? VL_STAGE_FRAG
+                      : cfg->precision == VL_FP64    ? VL_STAGE_GEN
+                      : c->use_tma                   ? VL_STAGE_TMA
+                                                     : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
         if (env) {
