@@ -147,6 +147,45 @@ def test_rhs_against_oracle_all_orders(cuda, n, precision):
     assert rel_err(rho, vo.moment_zero(f, c)) < 1e-13
 
 
+@pytest.mark.parametrize("n", [3, 5, 7, 9])
+def test_odd_orders_on_aligned_rows(cuda, n):
+    """Odd orders on an even number of v elements: the rows hold (nv + 2) n doubles, an even
+    count, so the FP64 stage kernel runs in its TMA form (odd rows are only 8-byte aligned on
+    other grids).  RHS of a random state and the three RK stage kinds against the oracle."""
+    from vlasov1d2v_b200 import _lib, problem
+    from vlasov1d2v_b200.context import get_context
+
+    res = (2, 3, 4)
+    p = problem.build(res, n, perturbation=None, amp=0.0)
+    c = vo.make_case(*res, n)
+    rng = np.random.default_rng(300 + n)
+    f = rng.standard_normal(c.shape)
+    E = rng.standard_normal((res[0] + 2, n))
+    p.elliptic.electric_field = torch.as_tensor(E, device="cuda")
+    r = _np(p.flux.semi_discrete_rhs(function=torch.as_tensor(f, device="cuda"),
+                                     elliptic=p.elliptic, basis=p.basis, grids=p.grids))[INNER]
+    R = vo.rhs(f, E, c)
+    assert rel_err(r, R[INNER]) < 1e-13
+    ctx = get_context(p.grids, accel=p.refs.electron_acceleration_multiplier,
+                      bfield=p.elliptic.magnetic_field, kappa=p.elliptic.poisson_coefficient,
+                      courant=p.stepper.courant)
+    fin = f.copy()
+    fin[0], fin[-1] = fin[-2], fin[1]  # periodic x ghosts: stage semantics
+    R = vo.rhs(fin, E, c)
+    fn = rng.standard_normal(c.shape)
+    dt = 0.0071
+    tin = torch.as_tensor(fin, device="cuda")
+    tfn = torch.as_tensor(fn, device="cuda")
+    tE = torch.as_tensor(E, device="cuda")
+    tdt = torch.tensor([dt], dtype=torch.float64, device="cuda")
+    for stage, want in ((0, fin + dt * R), (1, 0.75 * fn + 0.25 * fin + (0.25 * dt) * R),
+                        (2, fn / 3 + (2 / 3) * fin + ((2 / 3) * dt) * R)):
+        out = torch.zeros_like(tin)
+        ctx.rk_stage(stage, tin, tfn if stage else None, out, tE, tdt, xhalo=_lib.VL_XHALO_PERIODIC,
+                     partials=ctx.workspace)
+        assert rel_err(_np(out)[INNER], want[INNER]) < 1e-14
+
+
 def test_rk_stage_entry_point(cuda):
     """vl_rk_stage (one fused stage) against the oracle's stage formula."""
     from vlasov1d2v_b200 import _lib, problem
