@@ -10,6 +10,10 @@ Each state buffer (377 MB FP64 / 189 MB FP32) is larger than the 126 MB L2, so n
 needed between steps.  With N > 1 ranks (torchrun) every GPU advances its own replica (the
 solver is single-GPU; replicas only): ``value`` is the sum over ranks, times are the max.
 
+Variants in the same line: the FP32 mixed form of the same step, the large configuration
+(64^3 elements, n = 9, 191M DOF; both precisions; single-GPU runs only) and the 64-member
+heterogeneous FP32 ensemble.
+
 Prints ONE JSON line (rank 0).
 """
 import argparse
@@ -39,6 +43,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the batched-ensemble variant (64 heterogeneous FP32 members)")
     ap.add_argument("--ensemble-steps", type=int, default=50)
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the large-configuration variant (64^3 elements, n = 9)")
     ap.add_argument("--kernel-reps", type=int, default=10)
     ap.add_argument("--kernel-only", action="store_true",
                     help="launch each stage kind --kernel-reps times on --res (profiling target)")
@@ -253,20 +259,22 @@ def measured_peak_hbm():
         return 6650.0, "fallback 6.65 TB/s (of fallback)"
 
 
-def measure_precision(precision, steps, warmup, reps, dist):
+def measure_precision(precision, steps, warmup, reps, dist, res=None, order=None, e2e=True):
     import torch
 
     from vlasov1d2v_b200 import problem
     from vlasov1d2v_b200.timestep import _BIG_STEPS, get_max_speeds
 
-    p = problem.build(RES, ORDER, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=0,
+    res = tuple(res or RES)
+    order = order or ORDER
+    p = problem.build(res, order, perturbation="cos", amp=1.0e-3, noise=1.0e-6, seed=0,
                       precision=precision, batch_steps=max(steps, warmup, 1))
     st = p.stepper
     st.adapt_time_step(max_speeds=get_max_speeds(p.grids, p.elliptic, p.refs),
                        dx=p.grids.x.dx, du=p.grids.u.dx, dv=p.grids.v.dx)
     run = st._run(p.f, p.elliptic, p.grids, p.refs)
     run.upload_state(st._host_state(run, float("inf"), _BIG_STEPS))
-    n_dof = dof(RES, ORDER)
+    n_dof = dof(res, order)
     es = 8 if precision == "fp64" else 4
 
     # warm-up (eager), then capture the K-step graph
@@ -312,7 +320,7 @@ def measure_precision(precision, steps, warmup, reps, dist):
         torch.cuda.synchronize()
         stage_ms.append(a.elapsed_time(b) / reps)
     # field kernel (single CTA Poisson solve from a density)
-    rho = torch.zeros((RES[0], ORDER), dtype=torch.float64, device=run.f.device)
+    rho = torch.zeros((res[0], order), dtype=torch.float64, device=run.f.device)
     ctx.moment(run.f, rho)
     chg = (rho.mean() - rho).contiguous()
     phi = torch.empty_like(rho)
@@ -327,6 +335,12 @@ def measure_precision(precision, steps, warmup, reps, dist):
     torch.cuda.synchronize()
     field_ms = a.elapsed_time(b) / reps
 
+    state_bytes = run.f.numel() * es
+    if not e2e:
+        del g
+        return {"precision": precision, "ms": ms, "steps": steps, "dof": n_dof, "bytes_per_dof_step": 8 * es,
+                "stage_ms": stage_ms, "field_ms": field_ms, "state_bytes": state_bytes,
+                "stage_bytes": [2 * es * n_dof, 3 * es * n_dof, 3 * es * n_dof]}
     # end to end through the public API with host buffers: pinned f0 -> device, K steps,
     # device -> host of the final state and of the per-step energy/time/dt histories
     host_f = torch.empty(run.f.shape, dtype=run.f.dtype, pin_memory=True)
@@ -351,6 +365,26 @@ def measure_precision(precision, steps, warmup, reps, dist):
         "stage_ms": stage_ms, "field_ms": field_ms, "e2e_ms": e2e_ms, "state_bytes": state_bytes,
         "stage_bytes": [2 * es * n_dof, 3 * es * n_dof, 3 * es * n_dof],
     }
+
+
+LARGE_RES, LARGE_ORDER = (64, 64, 64), 9
+
+
+def measure_large(steps, warmup, dist, peak):
+    """The large benchmark configuration (64^3 elements, n = 9, 191M DOF; FP64 plain and FP32
+    mixed): DOF-updates/s of the graph-replayed step and each stage kernel's fraction of the HBM
+    roofline (the FP64 stage kernel is the generic kernel's TMA form, the FP32 one the
+    register-pencil kernel)."""
+    out = {"workload": "large loss-cone config: Nx=Nu=Nv=64, n=9 (576^3 = 191.1M DOF), "
+                       "1e-3 cos kx + 1e-6 noise"}
+    for prec in ("fp64", "fp32"):
+        r = measure_precision(prec, steps, warmup, 3, dist, res=LARGE_RES, order=LARGE_ORDER, e2e=False)
+        ms_step = r["ms"] / steps
+        fr = [b / (t * 1e-3) / (peak * 1e9) for b, t in zip(r["stage_bytes"], r["stage_ms"])]
+        out[prec] = {"value": r["dof"] / (ms_step * 1e-3), "unit": "DOF-updates/s", "ms_per_step": ms_step,
+                     "stage_ms": r["stage_ms"], "stage_roofline_frac": fr,
+                     "step_roofline_frac": r["bytes_per_dof_step"] * r["dof"] / (ms_step * 1e-3) / (peak * 1e9)}
+    return out
 
 
 def replica_throughput(dist, ms, steps, dof):
@@ -495,6 +529,11 @@ def main():
                                     "roofline": out["fp32"]["roofline"], "e2e": out["fp32"]["e2e"],
                                     "speedup_vs_fp64": out["fp32"]["value"] / head["value"]}},
     }
+    if not args.no_large and world == 1:
+        try:
+            line["variants"]["large_n9"] = measure_large(min(args.steps, 10), args.warmup, dist, peak)
+        except Exception as exc:   # the headline line is still printed
+            line["variants"]["large_n9"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_ensemble:
         try:
             line["variants"]["ensemble_fp32"] = measure_ensemble(args.ensemble_steps, args.warmup)
