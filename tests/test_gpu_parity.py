@@ -186,6 +186,42 @@ def test_odd_orders_on_aligned_rows(cuda, n):
         assert rel_err(_np(out)[INNER], want[INNER]) < 1e-14
 
 
+@pytest.mark.parametrize("res", [(2, 2, 3), (2, 2, 4)])
+@pytest.mark.parametrize("n", [3, 5, 7, 9])
+def test_fp32_phased_rows(cuda, n, res, monkeypatch):
+    """FP32 odd orders whose rows are not 16-byte multiples ((nv + 2) n floats) but whose rows of
+    one j share a 16-byte phase ((nu + 2) n (nv + 2) n a multiple of 4): the generic kernel's
+    phased form.  The three RK stage kinds of a random state against the FP64 oracle, within
+    FP32 rounding of the stage results.  The form is opt-in (VLASOV1D2V_GEN_PH=1, read when the
+    context is created)."""
+    from vlasov1d2v_b200 import _lib, problem
+    from vlasov1d2v_b200.context import get_context
+
+    monkeypatch.setenv("VLASOV1D2V_GEN_PH", "1")
+    p = problem.build(res, n, perturbation=None, amp=0.0, precision="fp32")
+    c = vo.make_case(*res, n)
+    ctx = get_context(p.grids, precision="fp32", accel=p.refs.electron_acceleration_multiplier,
+                      bfield=p.elliptic.magnetic_field, kappa=p.elliptic.poisson_coefficient,
+                      courant=p.stepper.courant)
+    rng = np.random.default_rng(500 + n + res[2])
+    fin = rng.standard_normal(c.shape).astype(np.float32).astype(np.float64)
+    fin[0], fin[-1] = fin[-2], fin[1]  # periodic x ghosts: stage semantics
+    fn = rng.standard_normal(c.shape).astype(np.float32).astype(np.float64)
+    E = rng.standard_normal((res[0] + 2, n))
+    R = vo.rhs(fin, E, c)
+    dt = 0.0071
+    tin = torch.as_tensor(fin, dtype=torch.float32, device="cuda")
+    tfn = torch.as_tensor(fn, dtype=torch.float32, device="cuda")
+    tE = torch.as_tensor(E, device="cuda")
+    tdt = torch.tensor([dt], dtype=torch.float64, device="cuda")
+    for stage, want in ((0, fin + dt * R), (1, 0.75 * fn + 0.25 * fin + (0.25 * dt) * R),
+                        (2, fn / 3 + (2 / 3) * fin + ((2 / 3) * dt) * R)):
+        out = torch.zeros_like(tin)
+        ctx.rk_stage(stage, tin, tfn if stage else None, out, tE, tdt, xhalo=_lib.VL_XHALO_PERIODIC,
+                     partials=ctx.workspace)
+        assert rel_err(_np(out).astype(np.float64)[INNER], want[INNER]) < 1e-5
+
+
 def test_rk_stage_entry_point(cuda):
     """vl_rk_stage (one fused stage) against the oracle's stage formula."""
     from vlasov1d2v_b200 import _lib, problem

@@ -269,6 +269,18 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                                 "stage_gen_tma_kernel");
         }
     }
+    if constexpr (sizeof(T) == 4) {
+        if (c->stage_kernel == VL_STAGE_GEN && c->gen_ph) {
+            using G = vl::GenPhGeom<N, float>;
+            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
+                 reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu)) % 16)
+                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
+            return check_launch(launch(c, vl::stage_gen_ph_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
+                                       tb),
+                                "stage_gen_ph_kernel");
+        }
+    }
     if (c->stage_kernel == VL_STAGE_GEN) {
         using G = vl::GenGeom<N, T>;
         // pair copies and stores of even orders need pair-aligned buffers
@@ -323,6 +335,17 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 template <int N, typename T>
 int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
     int blocks = 0;
+    if constexpr (sizeof(T) == 4) {
+        if (gen && gtma) {   // FP32: the phased form
+            using G = vl::GenPhGeom<N, float>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_gen_ph_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_ph_kernel<N>, G::THREADS,
+                                                              smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
+    }
     if constexpr (sizeof(T) == 8) {
         if (gen && gtma) {
             using G = vl::GenTmaGeom<N, double>;
@@ -703,9 +726,18 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     // FP64 the generic kernel for every other order (its TMA form where the rows allow); in FP32
     // the TMA kernel for n = 4 and the register-pencil kernel otherwise.
     // VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects one for comparisons
+    // FP32 on the generic kernel's phased form (all rows of one j share a 16-byte phase): opt-in
+    // with VLASOV1D2V_GEN_PH=1; measured within +-16% of the register-pencil kernel (faster at
+    // n = 7, 9, slower at n = 5, 6), so the pencil kernel stays the FP32 default
+    const bool ph_ok = ((size_t)(cfg->nu + 2) * n * (size_t)(cfg->nv + 2) * n) % 4 == 0;
+    {
+        const char *env = getenv("VLASOV1D2V_GEN_PH");
+        c->gen_ph = cfg->precision == VL_FP32 && ph_ok && env && env[0] == '1';
+    }
     c->stage_kernel = c->use_frag                    ? VL_STAGE_FRAG
                       : cfg->precision == VL_FP64    ? VL_STAGE_GEN
                       : c->use_tma                   ? VL_STAGE_TMA
+                      : c->gen_ph                    ? VL_STAGE_GEN
                                                      : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
@@ -726,9 +758,10 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         c->gen_tma = gen && cfg->precision == VL_FP64 && ((size_t)(cfg->nv + 2) * n) % 2 == 0 &&
                      encode_fn() != nullptr && !(env && env[0] == '1');
     }
+    c->gen_ph = c->gen_ph && gen;
     const int occ = cfg->precision == VL_FP64
                         ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma)
-                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, false);
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_ph);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double

@@ -32,7 +32,15 @@
 // completing on an mbarrier (bounded waits).  Rows are then contiguous copies of the state: the
 // tile starts at the 16-byte boundary at or below the left v trace, element b's node k sits at
 // column off + 1 + b n + k (off = 0 or 1 per tile), and the column pairs are read as two scalar
-// loads.  Every box lands on a 128-byte-aligned shared-memory address.  Row lengths hold an odd number of 16-byte units and planes an odd number of rows, so
+// loads.  Every box lands on a 128-byte-aligned shared-memory address.
+//
+// Phased form (FP32 rows that are not 16-byte multiples): every thread copies 16-byte chunks
+// with cp.async into contiguous rows, each row starting at the 16-byte boundary at or below the
+// tile's left v trace.  The offset of that trace inside the row ("phase", 0-3 floats) depends on
+// the row's position in the state; when (nu+2) n (nv+2) n is a multiple of 4 all rows of one j
+// (input, f^n, x faces, background) share one phase, (K0 + j (nv+2) n) mod 4 with K0 fixed per
+// tile, and the two u-face rows have their own.  The compute adds that per-j offset to its
+// columns and reads the pairs as two scalar loads.  Row lengths hold an odd number of 16-byte units and planes an odd number of rows, so
 // the loads of eight x nodes at one column fall in distinct banks.
 #pragma once
 
@@ -198,8 +206,38 @@ struct GenTmaGeom {
     static_assert(WB <= 256, "TMA box width");
 };
 
-// shared-memory layout constants of the two forms (row lengths, plane strides, array bytes)
-template <bool TMA, int N, typename T, int EPT>
+template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
+struct GenPhGeom {
+    static_assert(sizeof(T) == 4, "the phased form serves FP32 states");
+    static constexpr int EPT = EPT_;
+    static constexpr int WC = EPT * N + 2;                       // columns needed: tile + both traces
+    static constexpr int RS0 = (WC + 3 + 3) / 4 * 4;             // row slot: any phase, 16-byte units
+    static constexpr int RS = ((N * RS0 / 4) % 2 == 1) ? RS0 : RS0 + 4;   // odd 16-byte units per plane
+    static constexpr int PS = N * RS;
+    static constexpr int THREADS = GenGeom<N, T, EPT>::THREADS;
+    static constexpr int NST = 2;
+    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
+    static constexpr size_t IN_B = al(sizeof(T) * (size_t)N * PS);
+    static constexpr size_t FN_B = IN_B;
+    static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * N * RS);
+    static constexpr size_t UF_B = XF_B;
+    static constexpr size_t BG_B = al(sizeof(float) * (size_t)2 * N * RS);
+    static constexpr size_t UX_B = al(sizeof(double) * (size_t)N);
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
+    static constexpr size_t smem_bytes() {
+        const size_t s = NST * STAGE_B;
+        const size_t red = sizeof(dd) * (size_t)THREADS;
+        return (s > red ? s : red) + 128;
+    }
+    static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
+    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * 128);
+    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
+    static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
+};
+
+// shared-memory layout constants of the three forms (row lengths, plane strides, array bytes):
+// MODE 0 slot rows (cp.async), 1 TMA rows, 2 phased rows (cp.async)
+template <int MODE, int N, typename T, int EPT>
 struct GenLayout {
     using GG = GenGeom<N, T, EPT>;
     static constexpr int RIN = GG::W, PIN = GG::PS, RFN = GG::WN, PFN = GG::PSF, RFC = GG::WF, Q = 1;
@@ -208,7 +246,15 @@ struct GenLayout {
     static constexpr size_t S_BG = GG::BG_B, S_STAGE = GG::STAGE_B;
 };
 template <int N, typename T, int EPT>
-struct GenLayout<true, N, T, EPT> {
+struct GenLayout<2, N, T, EPT> {
+    using GP = GenPhGeom<N, T, EPT>;
+    static constexpr int RIN = GP::RS, PIN = GP::PS, RFN = GP::RS, PFN = GP::PS, RFC = GP::RS, Q = 4;
+    static constexpr int FS = N * GP::RS;
+    static constexpr size_t S_IN = GP::IN_B, S_FN = GP::FN_B, S_XF = GP::XF_B, S_UF = GP::UF_B;
+    static constexpr size_t S_BG = GP::BG_B, S_STAGE = GP::STAGE_B;
+};
+template <int N, typename T, int EPT>
+struct GenLayout<1, N, T, EPT> {
     using GT = GenTmaGeom<N, T, EPT>;
     static constexpr int RIN = GT::WB, PIN = GT::PS, RFN = GT::WB, PFN = GT::PS, RFC = GT::WB, Q = GT::Q;
     static constexpr int FS = (int)(GT::FSIDE_B / sizeof(T));
@@ -231,16 +277,17 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB, bool TMA = false>
+template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PH = false>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
                                                int g, int G, unsigned char *smem,
                                                const GenMaps *maps = nullptr) {
+    constexpr bool CONTIG = TMA || PH;   // contiguous rows (scalar pair loads)
     using GG = GenGeom<N, T, EPT>;
     using V2 = typename GenPair<T>::V;
     constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
     constexpr int PS = GG::PS, PSF = GG::PSF, NST = GG::NST, NW = GG::NW, NT = GG::THREADS;
     // shared-memory geometry of the form in use (TMA: contiguous rows of the state)
-    using L = GenLayout<TMA, N, T, EPT>;
+    using L = GenLayout<TMA ? 1 : (PH ? 2 : 0), N, T, EPT>;
     constexpr int RIN = L::RIN;      // IN row length
     constexpr int PIN = L::PIN;      // IN plane stride
     constexpr int RFN = L::RFN;      // FN row length
@@ -376,6 +423,60 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         }
         if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
     };
+    // phased form: 16-byte chunks of each row from the 16-byte boundary at or below the tile's
+    // left v trace through its right v trace (at most 3 floats more, still inside the array: the
+    // row after the last one read always exists); a warp per row.  VN = (nv + 2) n floats per row, base pointers 16-byte aligned.
+    auto issue_ph = [&](int s, int tt) {
+        if constexpr (PH) {
+            using GP = GenPhGeom<N, T, EPT>;
+            const int au = tt / nbt;
+            const int b0 = (tt - au * nbt) * EPT;
+            const int nb = min(EPT, nv - b0);
+            const int Ag = au + 1;
+            const size_t cg0 = (size_t)(b0 + 1) * N - 1;
+            const int wc = nb * N + 2;   // the tile's elements and both v traces (<= GP::WC)
+            unsigned char *st = stage_ptr(s);
+            T *dIn = reinterpret_cast<T *>(st);
+            T *dFn = reinterpret_cast<T *>(st + S_IN);
+            T *dXF = reinterpret_cast<T *>(st + S_IN + S_FN);
+            T *dUF = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF);
+            float *dBG = reinterpret_cast<float *>(st + S_IN + S_FN + S_XF + S_UF);
+            double *dUX = reinterpret_cast<double *>(st + S_IN + S_FN + S_XF + S_UF + S_BG);
+            // row r of a [rows][VN] array starting at base: the needed run from column cg0
+            auto row = [&](T *dst, const T *base, size_t r) {
+                const size_t A0 = r * (size_t)sJ + cg0;
+                const size_t S0 = A0 & ~(size_t)3;
+                const int nch = (int)((A0 - S0 + wc + 3) >> 2);
+                for (int k = lane; k < nch; k += 32) cp_async<16>(dst + 4 * k, base + S0 + 4 * k);
+            };
+            // row index of (e, i, a, j) in the state
+            auto sr = [&](int ee, int ii, int aa, int jj) -> size_t {
+                return (((size_t)ee * N + ii) * U + aa) * N + jj;
+            };
+            for (int r = warp; r < N * N; r += NW) {
+                const int ii = r / N, jj = r - ii * N;
+                row(dIn + ii * GP::PS + jj * GP::RS, in, sr(Eg, ii, Ag, jj));
+                if (with_fn) row(dFn + ii * GP::PS + jj * GP::RS, fn, sr(Eg, ii, Ag, jj));
+            }
+            for (int r = warp; r < 4 * N; r += NW) {
+                const int side = (r / N) & 1, q = r % N;
+                if (r < 2 * N)   // x traces: row j = q of (El, i = n-1) / (Er, i = 0)
+                    row(dXF + (side * N + q) * GP::RS, in, sr(side ? Er : El, side ? 0 : N - 1, Ag, q));
+                else             // u traces: row i = q of (a-1, j = n-1) / (a+1, j = 0)
+                    row(dUF + (side * N + q) * GP::RS, in, sr(Eg, q, side ? Ag + 1 : Ag - 1, side ? 0 : N - 1));
+            }
+            if (with_bg) {
+                for (int r = warp; r < 2 * N; r += NW) {
+                    const int tbl = r / N, jj = r % N;
+                    row(dBG + (tbl * N + jj) * GP::RS, tbl ? a.bg_rb : a.bg_eu, (size_t)Ag * N + jj);
+                }
+            }
+            if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
+        } else {
+            (void)s;
+            (void)tt;
+        }
+    };
     // TMA form: one thread loads the tile's boxes into stage s
     auto issue_tma = [&](int s, int tt) {
         if constexpr (TMA) {
@@ -428,14 +529,24 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     } else {
 #pragma unroll
         for (int s0 = 0; s0 < NST - 1; ++s0) {
-            if (s0 < ntile) issue(s0, g + s0 * G);
+            if (s0 < ntile) {
+                if constexpr (PH)
+                    issue_ph(s0, g + s0 * G);
+                else
+                    issue(s0, g + s0 * G);
+            }
             cp_async_commit();
         }
     }
     for (int q = 0; q < ntile; ++q) {
         if constexpr (!TMA) {
             const int qn = q + NST - 1;
-            if (qn < ntile) issue(qn % NST, g + qn * G);
+            if (qn < ntile) {
+                if constexpr (PH)
+                    issue_ph(qn % NST, g + qn * G);
+                else
+                    issue(qn % NST, g + qn * G);
+            }
             cp_async_commit();
         }
         const int tt = g + q * G;
@@ -465,12 +576,24 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         // column of element b's node 0 in the IN rows, of the thread's pair in IN and in the
         // FN / face / background rows; first u node in sUX
         const int cL = (b0 + 1) * N - 1;
-        const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : H + b * SL;
+        const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : (PH ? 1 + b * N : H + b * SL);
         const int cin = ebase + 2 * p;
-        const int cfc = TMA ? cin : cs;
+        const int cfc = CONTIG ? cin : cs;
+        // phased form: offset of the rows of index j (input, f^n, x faces, background) and of
+        // the two u-face rows inside their slots
+        const int K0 = (int)(((unsigned)Ag * (unsigned)N * (unsigned)sJ + (unsigned)cL) & 3u);
+        const int KJ = sJ & 3;
+        auto jsh = [&](int jj) -> int {
+            if constexpr (PH)
+                return (K0 + jj * KJ) & 3;
+            else
+                return 0;
+        };
+        const int ush0 = PH ? ((K0 - KJ) & 3) : 0;
+        const int ush1 = PH ? ((K0 + N * KJ) & 3) : 0;
         const double *sUX = sUX0 + (TMA ? ((Ag * N) & 1) : 0);
         auto ld2 = [&](const T *q2) -> V2 {
-            if constexpr (TMA) {
+            if constexpr (CONTIG) {
                 V2 r;
                 r.x = q2[0];
                 r.y = q2[1];
@@ -485,9 +608,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             const T sp0 = (T)sd0, sp1 = (T)sd1;
             V2 fu[N];
 #pragma unroll
-            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin);
-            const V2 ufl = ld2(sUF + i * RFC + cfc);
-            const V2 ufr = ld2(sUF + FS + i * RFC + cfc);
+            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin + jsh(m));
+            const V2 ufl = ld2(sUF + i * RFC + cfc + ush0);
+            const V2 ufr = ld2(sUF + FS + i * RFC + cfc + ush1);
             const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
             const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
             T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
@@ -499,7 +622,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 const bool xpos = uxd >= 0.0;
                 const bool vpos = svd >= 0.0;
                 // x: sum_m up[i][m] F[m][j][k] + lifts
-                const T *pc = sIn + j * RIN + cin;
+                const T *pc = sIn + j * RIN + cin + jsh(j);
                 T dx0 = (T)0, dx1 = (T)0;
                 V2 cm0, cmL;
 #pragma unroll
@@ -510,8 +633,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     dx0 = fma(upi[m], cv.x, dx0);
                     dx1 = fma(upi[m], cv.y, dx1);
                 }
-                const V2 xf0 = ld2(sXF + j * RFC + cfc);
-                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc);
+                const V2 xf0 = ld2(sXF + j * RFC + cfc + jsh(j));
+                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc + jsh(j));
                 const V2 xl = xpos ? xf0 : cm0;
                 const V2 xr = xpos ? cmL : xf1;
                 dx0 = fma(xig0, xl.x, dx0);
@@ -519,7 +642,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 dx1 = fma(xig0, xl.y, dx1);
                 dx1 = fma(-xig1, xr.y, dx1);
                 // v: sum_m F[i][j][m] up[k][m] + lifts (the element's k-line)
-                const T *pa = prow + j * RIN;
+                const T *pa = prow + j * RIN + jsh(j);
                 T line[2 * P];
 #pragma unroll
                 for (int m2 = 0; m2 < P; ++m2) {
@@ -533,8 +656,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     dv0 = fma(upk0[m], line[m], dv0);
                     dv1 = fma(upk1[m], line[m], dv1);
                 }
-                const T tl = vpos ? pa[TMA ? -1 : LH - H] : line[0];
-                const T tr = vpos ? line[N - 1] : pa[TMA ? N : SL];
+                const T tl = vpos ? pa[CONTIG ? -1 : LH - H] : line[0];
+                const T tr = vpos ? line[N - 1] : pa[CONTIG ? N : SL];
                 dv0 = fma(xik00, tl, dv0);
                 dv0 = fma(-xik01, tr, dv0);
                 dv1 = fma(xik10, tl, dv1);
@@ -554,8 +677,15 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
                 T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
                 if (with_bg) {   // RHS of the x-independent background
-                    const float2 eu = *reinterpret_cast<const float2 *>(sBG + j * RFC + cfc);
-                    const float2 rb = *reinterpret_cast<const float2 *>(sBG + N * RFC + j * RFC + cfc);
+                    float2 eu, rb;
+                    const float *pbg = sBG + j * RFC + cfc + jsh(j);
+                    if constexpr (CONTIG) {
+                        eu = make_float2(pbg[0], pbg[1]);
+                        rb = make_float2(pbg[N * RFC], pbg[N * RFC + 1]);
+                    } else {
+                        eu = *reinterpret_cast<const float2 *>(pbg);
+                        rb = *reinterpret_cast<const float2 *>(pbg + N * RFC);
+                    }
                     r0 += (T)fmaf((float)Ei, eu.x, rb.x);
                     r1 += (T)fmaf((float)Ei, eu.y, rb.y);
                 }
@@ -568,7 +698,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     o.x = fma(dtT, r0, fij.x);
                     o.y = fma(dtT, r1, fij.y);
                 } else {
-                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc);
+                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc + jsh(j));
                     o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
                     o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
                 }
@@ -627,6 +757,20 @@ stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
     gen_stage_body<N, T, GenGeom<N, T>::EPT>(a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
+}
+
+// phased form (FP32 rows that are not 16-byte multiples)
+template <int N>
+__global__ void __launch_bounds__(GenPhGeom<N, float>::THREADS, GenPhGeom<N, float>::MINB)
+stage_gen_ph_kernel(const StageArgs a, const __grid_constant__ StageTables<float> tb) {
+    pdl_wait();
+    pdl_trigger();
+    if (a.state != nullptr && a.state->active == 0) return;
+    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
+    gen_stage_body<N, float, GenGeom<N, float>::EPT, StageTables<float>, false, true>(
+        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
 // TMA form (FP64, 16-byte-aligned state rows)
