@@ -153,6 +153,19 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
 #pragma unroll
         for (int jc = 0; jc < JC; ++jc) ux[jc] = a.u_nodes[Ag * N + (jc < JN ? J0 + jc : 0)];
         const double vnode = act ? a.v_nodes[col] : 0.0;
+        // background-split RHS tables at the lane's (j, column): the same for every x node, so
+        // read once per tile
+        float beu[JC], brb[JC];
+#pragma unroll
+        for (int jc = 0; jc < JC; ++jc) {
+            beu[jc] = 0.0f;
+            brb[jc] = 0.0f;
+            if (a.bg_rb != nullptr && act && jc < JN) {
+                const int vi = Ag * sA + (J0 + jc) * sJ + col;
+                beu[jc] = a.bg_eu[vi];
+                brb[jc] = a.bg_rb[vi];
+            }
+        }
 
         // ---- own pencil columns (x lines) and the x upwind traces ----
         T f[N][JC];
@@ -279,10 +292,8 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
                 dv = fma(xik0, vL, dv);
                 dv = fma(-xik1, vR, dv);
                 T r = fma((T)ux[jc] * dx, jx, fma(s * du, ju, ((T)sv_d * dv) * jv));
-                if (a.bg_rb != nullptr) {   // RHS of the x-independent background
-                    const int vi = Ag * sA + j * sJ + col;
-                    r += (T)fmaf((float)sE[i], a.bg_eu[vi], a.bg_rb[vi]);
-                }
+                if (a.bg_rb != nullptr)   // RHS of the x-independent background
+                    r += (T)fmaf((float)sE[i], beu[jc], brb[jc]);
                 const T fij = rp[j * RW];
                 T o;
                 if (kind == KIND_RHS) {
