@@ -153,6 +153,18 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
 #pragma unroll
         for (int jc = 0; jc < JC; ++jc) ux[jc] = a.u_nodes[Ag * N + (jc < JN ? J0 + jc : 0)];
         const double vnode = act ? a.v_nodes[col] : 0.0;
+        // x and v flux speeds of the lane's j rows times their Jacobians, and their upwind
+        // directions: the same for every x node, so formed once per tile
+        T uxj[JC], svj[JC];
+        bool xposj[JC], vposj[JC];
+#pragma unroll
+        for (int jc = 0; jc < JC; ++jc) {
+            const double sv_d = accel * (nbfield * ux[jc]);
+            xposj[jc] = ux[jc] >= 0.0;
+            vposj[jc] = sv_d >= 0.0;
+            uxj[jc] = (T)ux[jc] * jx;
+            svj[jc] = (T)sv_d * jv;
+        }
         // background-split RHS tables at the lane's (j, column): the same for every x node, so
         // read once per tile
         float beu[JC], brb[JC];
@@ -264,7 +276,7 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
                 du = fma(tb.xi[2 * j], uL, du);
                 du = fma(-tb.xi[2 * j + 1], uR, du);
                 // x part: along i at column j (registers)
-                const bool xpos = ux[jc] >= 0.0;
+                const bool xpos = xposj[jc];
                 const T xL = xpos ? xh[jc] : f[0][jc];
                 const T xR = xpos ? f[N - 1][jc] : xh[jc];
                 T dx = (T)0;
@@ -276,8 +288,7 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
                 const T *lp = sF + (i * N + j) * RW + bl * N;
                 T line[N];
                 load_line<N, VEC, T>(lp, line);
-                const double sv_d = accel * (nbfield * ux[jc]);
-                const bool vpos = sv_d >= 0.0;
+                const bool vpos = vposj[jc];
                 T vL, vR;
                 if (vpos) {
                     vL = (bl > 0) ? lp[-1] : sVH[i * N + j];
@@ -291,7 +302,7 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
                 for (int m = 0; m < N; ++m) dv = fma(upk[m], line[m], dv);
                 dv = fma(xik0, vL, dv);
                 dv = fma(-xik1, vR, dv);
-                T r = fma((T)ux[jc] * dx, jx, fma(s * du, ju, ((T)sv_d * dv) * jv));
+                T r = fma(uxj[jc], dx, fma(s * du, ju, svj[jc] * dv));
                 if (a.bg_rb != nullptr)   // RHS of the x-independent background
                     r += (T)fmaf((float)sE[i], beu[jc], brb[jc]);
                 const T fij = rp[j * RW];
