@@ -213,7 +213,8 @@ size_t ens_smem(int threads) {
     size_t m = 0;
     for (int n = 1; n <= vl::NMAX; ++n) {
         const int rw = (32 / n) * n;
-        const size_t b = sizeof(double) * (size_t)n * threads + sizeof(T) * (size_t)(n * n * rw + n * n);
+        const size_t b = ((sizeof(double) * (size_t)n * threads + sizeof(T) * (size_t)(n * n * rw + n * n) + 7) &
+                          ~(size_t)7) + sizeof(double) * n;   // + the E values (vl::PencilGeom::se_offset)
         m = std::max(m, b);
     }
     return m;

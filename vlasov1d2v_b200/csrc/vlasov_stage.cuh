@@ -35,9 +35,11 @@ struct PencilGeom {
     static constexpr int MIN_BLOCKS = 65536 / (THREADS * REG_CAP) > 0 ? 65536 / (THREADS * REG_CAP) : 1;
     static constexpr int RW = EPW * N;                       // shared row length (v nodes)
     static constexpr int VEC = (sizeof(T) == 8) ? ((N % 2 == 0) ? 2 : 1) : ((N % 4 == 0) ? 4 : 1);
-    static constexpr size_t smem_bytes() {
-        return sizeof(double) * (size_t)(N * THREADS) + sizeof(T) * (size_t)(N * N * RW + N * N);
+    // [N][NT] moment partials, [N][N][RW] tile, [N][N] v traces, then [N] E values (8-aligned)
+    static constexpr size_t se_offset(int nt) {
+        return (sizeof(double) * (size_t)(N * nt) + sizeof(T) * (size_t)(N * N * RW + N * N) + 7) & ~(size_t)7;
     }
+    static constexpr size_t smem_bytes() { return se_offset(THREADS) + sizeof(double) * N; }
 };
 
 template <typename T, int VEC>
@@ -77,7 +79,7 @@ __device__ __forceinline__ void load_line(const T *p, T (&line)[N]) {
 // beyond ceil(N / JC_) have no j chunk and only take part in the barriers and loads of shared
 // data (the ensemble kernel runs several orders with one block size).  tb supplies up / xi
 // (compile-time indices: parameter or constant bank); qw the velocity weights (w_j w_k/(J_u J_v)).
-template <int N, typename T, int JC_, int NT_, typename TB>
+template <int N, typename T, int JC_, int NT_, typename TB, int J0C = -1>
 __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &tb, const double *qw,
                                                   int e, int g, int G) {
     using GP = PencilGeom<N, T>;
@@ -86,11 +88,13 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
     double *sMom = reinterpret_cast<double *>(smem_raw);            // [N][THREADS]
     T *sF = reinterpret_cast<T *>(sMom + N * NT);                   // [N][N][RW]
     T *sVH = sF + N * N * RW;                                       // [N][N]
-    __shared__ double sE[N];
+    double *sE = reinterpret_cast<double *>(smem_raw + GP::se_offset(NT));   // E at the x nodes
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int J0 = (tid >> 5) * JC;                 // warp-uniform j chunk
+    // warp-uniform j chunk; compile-time when the caller instantiates one body per warp, so the
+    // u-contraction coefficients up[j][m] become constant-bank operands
+    const int J0 = (J0C >= 0) ? J0C : (tid >> 5) * JC;
     const int JN = min(JC, N - J0);                 // <= 0: a warp without a j chunk
     const int bl = lane / N, k = lane - (lane / N) * N;
     const bool lane_ok = lane < EPW * N;
@@ -353,14 +357,28 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
     }
 }
 
+// one body instantiation per warp (its j chunk a template constant); every instantiation runs
+// the same sequence of barriers
+template <int N, typename T, int W>
+__device__ __forceinline__ void pencil_dispatch(const StageArgs &a, const StageTables<T> &tb, int w) {
+    using GP = PencilGeom<N, T>;
+    if constexpr (W < GP::JS) {
+        if (w == W) {
+            pencil_stage_body<N, T, GP::JC, GP::THREADS, StageTables<T>, W * GP::JC>(a, tb, tb.qw, blockIdx.y,
+                                                                                   blockIdx.x, gridDim.x);
+            return;
+        }
+        pencil_dispatch<N, T, W + 1>(a, tb, w);
+    }
+}
+
 template <int N, typename T>
 __global__ void __launch_bounds__(PencilGeom<N, T>::THREADS, PencilGeom<N, T>::MIN_BLOCKS)
 stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
     pdl_wait();
     pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
-    pencil_stage_body<N, T, PencilGeom<N, T>::JC, PencilGeom<N, T>::THREADS>(
-        a, tb, tb.qw, blockIdx.y, blockIdx.x, gridDim.x);
+    pencil_dispatch<N, T, 0>(a, tb, (int)(threadIdx.x >> 5));
 }
 
 }  // namespace vl
