@@ -256,7 +256,7 @@ VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, i
  *   vl_ens_bind       member i's state f, stage buffers, E, phi, loop state and workspace of
  *                     vl_ens_workspace_bytes(ens, i) bytes (the stage buffers' velocity ghosts
  *                     must equal f's, as for vl_ssp_rk3_steps)
- *   vl_ens_schedule   tunables: threads per CTA (64, 128 or 256), resident CTAs per SM, work items
+ *   vl_ens_schedule   tunables: threads per CTA (64 or 128), resident CTAs per SM, work items
  *                     per CTA (tile groups per x slab follow from it)
  *   vl_ens_commit     upload descriptors and the item list (synchronous; not inside a capture)
  *   vl_ens_steps      nsteps SSP-RK3 steps of every member (stream-ordered, capturable)      */

@@ -90,16 +90,8 @@ struct EnsJC {
     static constexpr int jc() { return (N + NT / 32 - 1) / (NT / 32); }
 };
 
-// resident CTAs the register allocation is sized for: the 64- and 128-thread forms keep the
-// registers of the largest order body (255, few spills, 8 warps per SM at most); the 256-thread
-// form (2 j values per thread at n = 9) is capped at 128 registers for two CTAs, 16 warps per SM
-template <int NT>
-struct EnsMinBlocks {
-    static constexpr int value = NT >= 256 ? 2 : 1;
-};
-
 template <typename T, int NT>
-__global__ void __launch_bounds__(NT, EnsMinBlocks<NT>::value) ens_stage_kernel(const EnsMember *__restrict__ members,
+__global__ void __launch_bounds__(NT) ens_stage_kernel(const EnsMember *__restrict__ members,
                                                       const int *__restrict__ cta_items,
                                                       const EnsItem *__restrict__ items, int stage) {
     __shared__ StageArgs sArgs;
@@ -121,8 +113,7 @@ __global__ void __launch_bounds__(NT, EnsMinBlocks<NT>::value) ens_stage_kernel(
 #define VL_ENS_CASE(NN)                                                                            \
     case NN:                                                                                       \
         pencil_stage_body<NN, T, EnsJC<NN>::template jc<NT>(), NT, EnsTables<T>>(                 \
-            sArgs, ens_tables<T>(NN), m.qw,                                                        \
-                                                                     item.e, item.g, m.G);         \
+            sArgs, ens_tables<T>(NN), m.qw, item.e, item.g, m.G);                                  \
         break;
             VL_ENS_CASE(1)
             VL_ENS_CASE(2)
@@ -231,12 +222,8 @@ int launch_stage(vl_ens *E, int stage, cudaStream_t s) {
 
 int stage(vl_ens *E, int st, cudaStream_t s) {
     if (E->precision == VL_FP64)
-        return E->threads == 64    ? launch_stage<double, 64>(E, st, s)
-               : E->threads == 128 ? launch_stage<double, 128>(E, st, s)
-                                   : launch_stage<double, 256>(E, st, s);
-    return E->threads == 64    ? launch_stage<float, 64>(E, st, s)
-           : E->threads == 128 ? launch_stage<float, 128>(E, st, s)
-                               : launch_stage<float, 256>(E, st, s);
+        return E->threads == 64 ? launch_stage<double, 64>(E, st, s) : launch_stage<double, 128>(E, st, s);
+    return E->threads == 64 ? launch_stage<float, 64>(E, st, s) : launch_stage<float, 128>(E, st, s);
 }
 
 int field(vl_ens *E, int kind, cudaStream_t s) {
@@ -378,17 +365,13 @@ VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out) {
         vl_ens_destroy(E);
         return efail(VL_ERR_CUDA, std::string("cudaMalloc(ensemble): ") + cudaGetErrorString(e));
     }
-    for (int t : {64, 128, 256}) {
+    for (int t : {64, 128}) {
         const size_t smem = E->precision == VL_FP64 ? ens_smem<double>(t) : ens_smem<float>(t);
         if (E->precision == VL_FP64)
-            cudaFuncSetAttribute(t == 64    ? vl::ens_stage_kernel<double, 64>
-                                 : t == 128 ? vl::ens_stage_kernel<double, 128>
-                                            : vl::ens_stage_kernel<double, 256>,
+            cudaFuncSetAttribute(t == 64 ? vl::ens_stage_kernel<double, 64> : vl::ens_stage_kernel<double, 128>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         else
-            cudaFuncSetAttribute(t == 64    ? vl::ens_stage_kernel<float, 64>
-                                 : t == 128 ? vl::ens_stage_kernel<float, 128>
-                                            : vl::ens_stage_kernel<float, 256>,
+            cudaFuncSetAttribute(t == 64 ? vl::ens_stage_kernel<float, 64> : vl::ens_stage_kernel<float, 128>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     *out = E;
@@ -481,8 +464,7 @@ VL_API int vl_ens_bind(vl_ens *E, int32_t i, void *f, void *sa, void *sb, double
 
 VL_API int vl_ens_schedule(vl_ens *E, int32_t threads, int32_t ctas_per_sm, int32_t items_per_cta) {
     if (!E) return efail(VL_ERR_INVALID, "null ensemble");
-    if (threads != 64 && threads != 128 && threads != 256)
-        return efail(VL_ERR_INVALID, "threads must be 64, 128 or 256");
+    if (threads != 64 && threads != 128) return efail(VL_ERR_INVALID, "threads must be 64 or 128");
     if (ctas_per_sm < 1 || ctas_per_sm > 32 || items_per_cta < 1 || items_per_cta > 64)
         return efail(VL_ERR_INVALID, "ctas_per_sm in 1..32, items_per_cta in 1..64");
     E->threads = threads;

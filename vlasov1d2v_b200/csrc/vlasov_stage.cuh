@@ -357,18 +357,18 @@ __device__ __forceinline__ void pencil_stage_body(const StageArgs &a, const TB &
     }
 }
 
-// one body instantiation per warp (its j chunk a template constant); every instantiation runs
-// the same sequence of barriers
-template <int N, typename T, int W>
-__device__ __forceinline__ void pencil_dispatch(const StageArgs &a, const StageTables<T> &tb, int w) {
-    using GP = PencilGeom<N, T>;
-    if constexpr (W < GP::JS) {
+// one body instantiation per warp w of an NT-thread CTA (its j chunk a template constant; warps
+// past the last chunk take part in the barriers only); every instantiation runs the same sequence
+// of barriers
+template <int N, typename T, int JC, int NT, typename TB, int W = 0>
+__device__ __forceinline__ void pencil_body_per_warp(const StageArgs &a, const TB &tb, const double *qw, int e,
+                                                     int g, int G, int w) {
+    if constexpr (W < NT / 32) {
         if (w == W) {
-            pencil_stage_body<N, T, GP::JC, GP::THREADS, StageTables<T>, W * GP::JC>(a, tb, tb.qw, blockIdx.y,
-                                                                                   blockIdx.x, gridDim.x);
+            pencil_stage_body<N, T, JC, NT, TB, (W * JC < N ? W * JC : N)>(a, tb, qw, e, g, G);
             return;
         }
-        pencil_dispatch<N, T, W + 1>(a, tb, w);
+        pencil_body_per_warp<N, T, JC, NT, TB, W + 1>(a, tb, qw, e, g, G, w);
     }
 }
 
@@ -378,7 +378,8 @@ stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb
     pdl_wait();
     pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
-    pencil_dispatch<N, T, 0>(a, tb, (int)(threadIdx.x >> 5));
+    pencil_body_per_warp<N, T, PencilGeom<N, T>::JC, PencilGeom<N, T>::THREADS, StageTables<T>>(
+        a, tb, tb.qw, blockIdx.y, blockIdx.x, gridDim.x, (int)(threadIdx.x >> 5));
 }
 
 }  // namespace vl

@@ -124,8 +124,8 @@ class Ensemble:
             self.set_schedule(*cache[key]["schedule"])
             return cache[key]
         if candidates is None:
-            candidates = [(t, c, k) for t in (256, 128, 64) for c in (1, 2, 3, 4) for k in (1, 2, 4, 8)
-                          if not (t == 128 and c > 2) and not (t == 256 and c > 2)]
+            candidates = [(t, c, k) for t in (128, 64) for c in (1, 2, 3, 4) for k in (1, 2, 4, 8)
+                          if not (t == 128 and c > 2)]
         snap = self._snapshot()
         trials = []
         try:
