@@ -23,8 +23,9 @@ def _build(q, precision, batch):
                          background_split=False, **q)
 
 
+@pytest.mark.parametrize("schedule", [None, (0, 0, 2)], ids=["fused", "by_order"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
-def test_ensemble_members_match_single_runs(cuda, precision, tol):
+def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
     from vlasov1d2v_b200.ensemble import Ensemble
 
     singles = []
@@ -35,6 +36,8 @@ def test_ensemble_members_match_single_runs(cuda, precision, tol):
         singles.append(p)
     probs = [_build(q, precision, 3) for q in MEMBERS]
     ens = Ensemble(probs, batch_steps=3)
+    if schedule is not None:
+        ens.set_schedule(*schedule)
     ens.run_steps(3)
     ens.run_steps(3, use_graph=False)
     for p, s in zip(probs, singles):
@@ -59,8 +62,9 @@ def test_ensemble_final_times_and_autotune(cuda):
     finals = [1e9, 2.5 * dt0[1], 1e9]
     ens = Ensemble(probs, final_time=finals, batch_steps=8)
     f_before = [p.f.arr.get().copy() for p in probs]
-    res = ens.autotune(candidates=[(128, 1, 1), (128, 2, 2), (64, 2, 4)], steps=2, cache_path=None)
-    assert res["schedule"] in [[128, 1, 1], [128, 2, 2], [64, 2, 4]] and len(res["trials"]) == 3
+    cands = [(128, 1, 1), (128, 2, 2), (64, 2, 4), (0, 0, 4)]
+    res = ens.autotune(candidates=cands, steps=2, cache_path=None)
+    assert res["schedule"] in [list(c) for c in cands] and len(res["trials"]) == 4
     for p, f0 in zip(probs, f_before):   # tuning restored the states
         np.testing.assert_array_equal(p.f.arr.get(), f0)
     ens.run_steps(8)

@@ -26,7 +26,7 @@ EXPORTED = (
     "vl_rk_stage", "vl_run_state_init", "vl_ssp_rk3_steps", "vl_sync_ghosts",
     "vl_ssp_rk3_steps_noalloc", "vl_initial_state", "vl_smooth_edges", "vl_interpolate",
     "vl_set_background", "vl_ens_create", "vl_ens_destroy", "vl_ens_workspace_bytes", "vl_ens_bind",
-    "vl_ens_schedule", "vl_ens_commit", "vl_ens_steps", "vl_mlp_dims", "vl_mlp_forward",
+    "vl_ens_schedule", "vl_ens_schedule_by_order", "vl_ens_commit", "vl_ens_steps", "vl_mlp_dims", "vl_mlp_forward",
     "vl_mlp_partial_floats", "vl_mlp_backward", "vl_mlp_adam", "vl_closure_features", "vl_closure_apply",
     "vl_poisson_dg", "vl_axpby_interior",
 )
@@ -110,6 +110,7 @@ def _declare(lib):
     lib.vl_ens_workspace_bytes.restype = ctypes.c_size_t
     lib.vl_ens_bind.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp]
     lib.vl_ens_schedule.argtypes = [vp, i32, i32, i32]
+    lib.vl_ens_schedule_by_order.argtypes = [vp, i32]
     lib.vl_ens_commit.argtypes = [vp]
     lib.vl_ens_steps.argtypes = [vp, i32, vp]
     f32, f64 = ctypes.c_float, ctypes.c_double

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <queue>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "vlasov_ctx.cuh"
@@ -130,6 +131,49 @@ __global__ void __launch_bounds__(NT) ens_stage_kernel(const EnsMember *__restri
     }
 }
 
+// Register cap of the by-order kernels.  The body reads its arguments from shared memory (they
+// differ per work item), not from the constant bank as the single-problem kernel does, and needs
+// more registers: at a cap of 128 the order-9 FP32 body spills 624 bytes; uncapped (255) it uses
+// 254 registers without spills and the 64-member benchmark ensemble steps in 4.09 ms against
+// 4.26 ms at a cap of 168 and 4.35 ms at 128.
+#ifndef VL_ENS_REG_CAP
+#define VL_ENS_REG_CAP 255
+#endif
+
+// resident CTAs per SM requested from the compiler for one order's kernel (register cap)
+template <int N, typename T>
+struct EnsOrderGeom {
+    static constexpr int THREADS = PencilGeom<N, T>::THREADS;
+    static constexpr int MIN_BLOCKS = 65536 / (THREADS * VL_ENS_REG_CAP) > 0 ? 65536 / (THREADS * VL_ENS_REG_CAP) : 1;
+};
+
+// The members of one order only, with that order's register-pencil geometry: its block size,
+// a register cap and one body instantiation per warp (the j chunk a template constant), so each
+// order gets its own register allocation instead of the largest order's.
+template <typename T, int N>
+__global__ void __launch_bounds__(EnsOrderGeom<N, T>::THREADS, EnsOrderGeom<N, T>::MIN_BLOCKS)
+ens_order_kernel(const EnsMember *__restrict__ members, const int *__restrict__ cta_items,
+                 const EnsItem *__restrict__ items, int stage) {
+    using GP = PencilGeom<N, T>;
+    __shared__ StageArgs sArgs;
+    __shared__ int sActive;
+    for (int it = cta_items[blockIdx.x]; it < cta_items[blockIdx.x + 1]; ++it) {
+        const EnsItem item = items[it];
+        const EnsMember &m = members[item.member];
+        __syncthreads();   // the previous item is done with the shared arguments and tiles
+        if (threadIdx.x == 0) {
+            StageArgs a = m.a;
+            ens_stage_args(a, m, stage);
+            sArgs = a;
+            sActive = (a.state == nullptr) || (a.state->active != 0);
+        }
+        __syncthreads();
+        if (!sActive) continue;
+        pencil_body_per_warp<N, T, GP::JC, GP::THREADS, EnsTables<T>>(sArgs, ens_tables<T>(N), m.qw, item.e,
+                                                                      item.g, m.G, (int)(threadIdx.x >> 5));
+    }
+}
+
 // field solves of all members: blockIdx.y = member, blockIdx.x = mode / node chunk
 __global__ void __launch_bounds__(FIELD_THREADS) ens_field_fwd_kernel(const FieldArgs *__restrict__ fa) {
     const FieldArgs &a = fa[blockIdx.y];
@@ -163,6 +207,12 @@ struct vl_ens {
     // schedule
     int threads = 128, ctas = 0;
     std::vector<int> G;
+    // by-order schedule: one stage launch per order present (ctas CTAs from cta_items[base])
+    struct Group {
+        int n, ctas, base;
+    };
+    bool by_order = false;
+    std::vector<Group> groups;
     vl::EnsMember *d_members = nullptr;
     vl::FieldArgs *d_field[3] = {nullptr, nullptr, nullptr};
     int *d_cta_items = nullptr;
@@ -220,7 +270,57 @@ int launch_stage(vl_ens *E, int stage, cudaStream_t s) {
     return VL_OK;
 }
 
+// resident CTAs per SM of one order's kernel (sets its dynamic shared-memory limit first)
+template <typename T, int N>
+int order_blocks(int *blocks) {
+    using GP = vl::PencilGeom<N, T>;
+    VL_ECUDA(cudaFuncSetAttribute(vl::ens_order_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)GP::smem_bytes()));
+    VL_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, vl::ens_order_kernel<T, N>, GP::THREADS,
+                                                           GP::smem_bytes()));
+    if (*blocks < 1) return efail(VL_ERR_CUDA, "ens_order_kernel: no resident CTA");
+    return VL_OK;
+}
+
+template <typename T, int N>
+int launch_order(vl_ens *E, const vl_ens::Group &g, int stage, cudaStream_t s) {
+    using GP = vl::PencilGeom<N, T>;
+    vl::ens_order_kernel<T, N><<<g.ctas, GP::THREADS, GP::smem_bytes(), s>>>(E->d_members, E->d_cta_items + g.base,
+                                                                              E->d_items, stage);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_order_kernel: ") + cudaGetErrorString(e));
+    return VL_OK;
+}
+
+// compile-time order from a runtime one: F is called with std::integral_constant<int, n>
+template <typename F>
+int with_order(int n, F &&f) {
+    switch (n) {
+        case 1: return f(std::integral_constant<int, 1>());
+        case 2: return f(std::integral_constant<int, 2>());
+        case 3: return f(std::integral_constant<int, 3>());
+        case 4: return f(std::integral_constant<int, 4>());
+        case 5: return f(std::integral_constant<int, 5>());
+        case 6: return f(std::integral_constant<int, 6>());
+        case 7: return f(std::integral_constant<int, 7>());
+        case 8: return f(std::integral_constant<int, 8>());
+        case 9: return f(std::integral_constant<int, 9>());
+        default: return efail(VL_ERR_UNSUPPORTED, "ensemble members take orders 1..9");
+    }
+}
+
 int stage(vl_ens *E, int st, cudaStream_t s) {
+    if (E->by_order) {
+        for (const vl_ens::Group &g : E->groups) {
+            const int rc = with_order(g.n, [&](auto nc) {
+                constexpr int N = decltype(nc)::value;
+                return E->precision == VL_FP64 ? launch_order<double, N>(E, g, st, s)
+                                               : launch_order<float, N>(E, g, st, s);
+            });
+            if (rc) return rc;
+        }
+        return VL_OK;
+    }
     if (E->precision == VL_FP64)
         return E->threads == 64 ? launch_stage<double, 64>(E, st, s) : launch_stage<double, 128>(E, st, s);
     return E->threads == 64 ? launch_stage<float, 64>(E, st, s) : launch_stage<float, 128>(E, st, s);
@@ -253,54 +353,71 @@ int upload_tables(const std::vector<vl_ctx *> &ctxs) {
     return VL_OK;
 }
 
+struct CostItem {
+    double cost;
+    vl::EnsItem it;
+};
+
+// longest processing time first onto the least-loaded of P CTAs; appends the CTAs' item ranges
+// (P + 1 offsets) and items
+void assign_lpt(std::vector<CostItem> &items, int P, std::vector<int> &offs, std::vector<vl::EnsItem> &flat) {
+    std::sort(items.begin(), items.end(), [](const CostItem &a, const CostItem &b) { return a.cost > b.cost; });
+    std::vector<std::vector<vl::EnsItem>> per(P);
+    using Load = std::pair<double, int>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int p = 0; p < P; ++p) heap.push({0.0, p});
+    for (const CostItem &it : items) {
+        Load l = heap.top();
+        heap.pop();
+        per[l.second].push_back(it.it);
+        heap.push({l.first + it.cost, l.second});
+    }
+    for (int p = 0; p < P; ++p) {
+        offs.push_back((int)flat.size());
+        flat.insert(flat.end(), per[p].begin(), per[p].end());
+    }
+    offs.push_back((int)flat.size());
+}
+
 // rebuild the device descriptors and the item list after a bind or schedule change
 int commit(vl_ens *E) {
     const int count = (int)E->ctx.size();
     for (int i = 0; i < count; ++i)
         if (!E->bound[i]) return efail(VL_ERR_INVALID, "ensemble member " + std::to_string(i) + " is not bound");
-    // item costs: tiles per item x n^3 (DOFs per tile ~ 32 n^2, contraction length n)
-    struct Item {
-        double cost;
-        vl::EnsItem it;
-    };
-    std::vector<Item> items;
+    // item costs: tiles per item x n^3 (DOFs per tile ~ 32 n^2, contraction length n); items of
+    // order n go to list n (by-order schedule) or all to list 0
+    std::vector<CostItem> items[vl::NMAX + 1];
     E->max_fwd = E->max_inv = 1;
     for (int i = 0; i < count; ++i) {
         const vl_ctx *c = E->ctx[i];
         const int G = E->G[i];
         const double n = c->cfg.n;
         const int tiles = tiles_of(c);
+        std::vector<CostItem> &list = items[E->by_order ? c->cfg.n : 0];
         for (int e = 0; e < c->cfg.nx; ++e)
             for (int g = 0; g < G; ++g) {
                 const int nt = (tiles - g + G - 1) / G;
-                items.push_back({nt * n * n * n, {i, e, g, 0}});
+                list.push_back({nt * n * n * n, {i, e, g, 0}});
             }
         E->members[i].G = G;
         for (int k = 0; k < 3; ++k) E->field[k][i].G = G;
         E->max_fwd = std::max(E->max_fwd, (c->cfg.n_modes + vl::FWD_MODES - 1) / vl::FWD_MODES);
         E->max_inv = std::max(E->max_inv, (c->cfg.nx * c->cfg.n + vl::INV_NODES - 1) / vl::INV_NODES);
     }
-    // longest processing time first onto the least-loaded CTA
-    std::sort(items.begin(), items.end(), [](const Item &a, const Item &b) { return a.cost > b.cost; });
-    const int P = std::max(1, std::min(E->ctas, (int)items.size()));
-    E->ctas = P;
-    std::vector<std::vector<vl::EnsItem>> per(P);
-    using Load = std::pair<double, int>;
-    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-    for (int p = 0; p < P; ++p) heap.push({0.0, p});
-    for (const Item &it : items) {
-        Load l = heap.top();
-        heap.pop();
-        per[l.second].push_back(it.it);
-        heap.push({l.first + it.cost, l.second});
-    }
-    std::vector<int> offs(P + 1, 0);
+    std::vector<int> offs;
     std::vector<vl::EnsItem> flat;
-    for (int p = 0; p < P; ++p) {
-        offs[p] = (int)flat.size();
-        flat.insert(flat.end(), per[p].begin(), per[p].end());
+    if (E->by_order) {
+        for (vl_ens::Group &g : E->groups) {
+            std::vector<CostItem> &list = items[g.n];
+            g.ctas = std::max(1, std::min(g.ctas, (int)list.size()));
+            g.base = (int)offs.size();
+            assign_lpt(list, g.ctas, offs, flat);
+        }
+    } else {
+        const int P = std::max(1, std::min(E->ctas, (int)items[0].size()));
+        E->ctas = P;
+        assign_lpt(items[0], P, offs, flat);
     }
-    offs[P] = (int)flat.size();
     cudaFree(E->d_cta_items);
     cudaFree(E->d_items);
     E->d_cta_items = nullptr;
@@ -467,6 +584,7 @@ VL_API int vl_ens_schedule(vl_ens *E, int32_t threads, int32_t ctas_per_sm, int3
     if (threads != 64 && threads != 128) return efail(VL_ERR_INVALID, "threads must be 64 or 128");
     if (ctas_per_sm < 1 || ctas_per_sm > 32 || items_per_cta < 1 || items_per_cta > 64)
         return efail(VL_ERR_INVALID, "ctas_per_sm in 1..32, items_per_cta in 1..64");
+    E->by_order = false;
     E->threads = threads;
     E->ctas = E->sm_count * ctas_per_sm;
     // split each member's x slabs into tile groups so that the item count is about
@@ -486,6 +604,46 @@ VL_API int vl_ens_schedule(vl_ens *E, int32_t threads, int32_t ctas_per_sm, int3
         int G = (int)(tiles * n * n * n / target + 0.5);
         E->G[i] = std::max(1, std::min(G, tiles));
     }
+    E->dirty = true;
+    return VL_OK;
+}
+
+VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta) {
+    if (!E) return efail(VL_ERR_INVALID, "null ensemble");
+    if (items_per_cta < 1 || items_per_cta > 64) return efail(VL_ERR_INVALID, "items_per_cta in 1..64");
+    const int count = (int)E->ctx.size();
+    double total[vl::NMAX + 1] = {};
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        const double n = c->cfg.n;
+        total[c->cfg.n] += (double)c->cfg.nx * tiles_of(c) * n * n * n;
+    }
+    // one group per order present, as many CTAs as its kernel keeps resident on the device
+    std::vector<vl_ens::Group> groups;
+    for (int n = vl::NMAX; n >= 1; --n) {
+        if (total[n] == 0.0) continue;
+        int blocks = 0;
+        const int rc = with_order(n, [&](auto nc) {
+            constexpr int N = decltype(nc)::value;
+            return E->precision == VL_FP64 ? order_blocks<double, N>(&blocks) : order_blocks<float, N>(&blocks);
+        });
+        if (rc) return rc;
+        groups.push_back({n, E->sm_count * blocks, 0});
+    }
+    // tile groups per member: about items_per_cta items of similar cost per CTA of its order
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        const double n = c->cfg.n;
+        int ctas = 1;
+        for (const vl_ens::Group &g : groups)
+            if (g.n == c->cfg.n) ctas = g.ctas;
+        const double target = total[c->cfg.n] / ((double)ctas * items_per_cta);
+        const int tiles = tiles_of(c);
+        const int G = (int)(tiles * n * n * n / target + 0.5);
+        E->G[i] = std::max(1, std::min(G, tiles));
+    }
+    E->groups = groups;
+    E->by_order = true;
     E->dirty = true;
     return VL_OK;
 }
