@@ -43,6 +43,11 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true",
                     help="skip the batched-ensemble variant (64 heterogeneous FP32 members)")
     ap.add_argument("--ensemble-steps", type=int, default=50)
+    ap.add_argument("--ensemble-only", action="store_true",
+                    help="measure the batched-ensemble variant alone (profiling target)")
+    ap.add_argument("--ensemble-schedule", type=int, nargs=3, default=None,
+                    metavar=("THREADS", "CTAS_PER_SM", "ITEMS_PER_CTA"),
+                    help="fixed ensemble schedule instead of the autotuner (threads 0: by order)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the large-configuration variant (64^3 elements, n = 9)")
     ap.add_argument("--kernel-reps", type=int, default=10)
@@ -118,7 +123,7 @@ def cpu_port_rate(steps, warmup):
     return dof(SAMPLE_RES, ORDER) / t, t, cores
 
 
-def measure_ensemble(steps, warmup, members=64, seed=0):
+def measure_ensemble(steps, warmup, members=64, seed=0, schedule=None):
     """Batched heterogeneous ensemble (64 seeded FP32 members, orders 6-9, up to 2.4M DOF each):
     aggregate DOF-updates/s of the ensemble driver (schedule from the autotuner), and of the same
     members stepped one after another through the single-problem loop (each graph-captured)."""
@@ -131,7 +136,11 @@ def measure_ensemble(steps, warmup, members=64, seed=0):
     probs = build_members(params, precision="fp32", seed=seed, batch_steps=max(steps, warmup))
     ens = Ensemble(probs, batch_steps=max(steps, warmup))
     setup_s = time.perf_counter() - t0
-    tune = ens.autotune(steps=3, use_cache=False, cache_path=None)
+    if schedule is None:
+        tune = ens.autotune(steps=3, use_cache=False, cache_path=None)
+    else:
+        ens.set_schedule(*schedule)
+        tune = {"schedule": list(schedule), "trials": []}
     total = ens.total_dof()
     ens.launch(warmup, use_graph=False)
     ens.launch(steps, use_graph=True)   # capture
@@ -430,6 +439,13 @@ def main():
     args = parse()
     if args.kernel_only:
         return kernel_only(args)
+    if args.ensemble_only:
+        import torch
+
+        torch.cuda.set_device(0)
+        res = measure_ensemble(args.ensemble_steps, args.warmup, schedule=args.ensemble_schedule)
+        print(json.dumps({"ensemble_only": True, "ensemble_fp32": res}))
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -536,7 +552,8 @@ def main():
             line["variants"]["large_n9"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_ensemble:
         try:
-            line["variants"]["ensemble_fp32"] = measure_ensemble(args.ensemble_steps, args.warmup)
+            line["variants"]["ensemble_fp32"] = measure_ensemble(args.ensemble_steps, args.warmup,
+                                                                 schedule=args.ensemble_schedule)
         except Exception as exc:  # the headline line must survive a failure of the extra
             line["variants"]["ensemble_fp32"] = {"error": f"{type(exc).__name__}: {exc}"}
     if not args.no_cpu_baseline and world == 1:

@@ -186,18 +186,22 @@ def test_odd_orders_on_aligned_rows(cuda, n):
         assert rel_err(_np(out)[INNER], want[INNER]) < 1e-14
 
 
+@pytest.mark.parametrize("form", ["pencil", "phased"])
 @pytest.mark.parametrize("res", [(2, 2, 3), (2, 2, 4)])
-@pytest.mark.parametrize("n", [3, 5, 7, 9])
-def test_fp32_phased_rows(cuda, n, res, monkeypatch):
-    """FP32 odd orders whose rows are not 16-byte multiples ((nv + 2) n floats) but whose rows of
-    one j share a 16-byte phase ((nu + 2) n (nv + 2) n a multiple of 4): the generic kernel's
-    phased form.  The three RK stage kinds of a random state against the FP64 oracle, within
-    FP32 rounding of the stage results.  The form is opt-in (VLASOV1D2V_GEN_PH=1, read when the
-    context is created)."""
+@pytest.mark.parametrize("n", [3, 5, 6, 7, 9])
+def test_fp32_stage_kernels_other_orders(cuda, n, res, form, monkeypatch):
+    """FP32 orders other than 4 and 8: the register-pencil kernel (the default there) and the
+    generic kernel's phased form, for rows that are not 16-byte multiples ((nv + 2) n floats) but
+    whose rows of one j share a 16-byte phase ((nu + 2) n (nv + 2) n a multiple of 4).  The three
+    RK stage kinds of a random state against the FP64 oracle, within FP32 rounding of the stage
+    results.  The phased form is opt-in (VLASOV1D2V_GEN_PH=1, read when the context is created)."""
     from vlasov1d2v_b200 import _lib, problem
     from vlasov1d2v_b200.context import get_context
 
-    monkeypatch.setenv("VLASOV1D2V_GEN_PH", "1")
+    if form == "phased":
+        monkeypatch.setenv("VLASOV1D2V_GEN_PH", "1")
+    else:
+        monkeypatch.delenv("VLASOV1D2V_GEN_PH", raising=False)
     p = problem.build(res, n, perturbation=None, amp=0.0, precision="fp32")
     c = vo.make_case(*res, n)
     ctx = get_context(p.grids, precision="fp32", accel=p.refs.electron_acceleration_multiplier,

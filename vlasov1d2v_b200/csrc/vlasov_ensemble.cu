@@ -136,25 +136,43 @@ __global__ void __launch_bounds__(NT) ens_stage_kernel(const EnsMember *__restri
 // more registers: at a cap of 128 the order-9 FP32 body spills 624 bytes; uncapped (255) it uses
 // 254 registers without spills and the 64-member benchmark ensemble steps in 4.09 ms against
 // 4.26 ms at a cap of 168 and 4.35 ms at 128.
+// order groups of a by-order stage launched on concurrent streams (1) or one after another (0)
+#ifndef VL_ENS_CONCURRENT
+#define VL_ENS_CONCURRENT 1
+#endif
+
 #ifndef VL_ENS_REG_CAP
 #define VL_ENS_REG_CAP 255
 #endif
 
-// resident CTAs per SM requested from the compiler for one order's kernel (register cap)
+// j values per thread of the FP32 by-order kernels (capped at the order): one warp per CTA with
+// all j rows for orders up to 8.  64-member FP32 ensemble, ms per step at 8 items per CTA: 3.99
+// with the single-problem kernel's 4 (two warps per CTA for orders 5..8), 3.24 with 8, 6.3 with
+// 2 and 10.8 with 1; the one-warp CTAs synchronise within a warp and hold more rows in registers.
+// FP64 keeps the single-problem kernel's 2.
+#ifndef VL_ENS_JC32
+#define VL_ENS_JC32 8
+#endif
+
+// block shape and resident CTAs per SM requested from the compiler for one order's kernel
 template <int N, typename T>
 struct EnsOrderGeom {
-    static constexpr int THREADS = PencilGeom<N, T>::THREADS;
+    static constexpr int JC0 = sizeof(T) == 4 ? (VL_ENS_JC32 < N ? VL_ENS_JC32 : N) : PencilGeom<N, T>::JC;
+    static constexpr int JS = (N + JC0 - 1) / JC0;              // warps (j chunks)
+    static constexpr int JC = (N + JS - 1) / JS;                // balanced chunk
+    static constexpr int THREADS = 32 * JS;
     static constexpr int MIN_BLOCKS = 65536 / (THREADS * VL_ENS_REG_CAP) > 0 ? 65536 / (THREADS * VL_ENS_REG_CAP) : 1;
+    static constexpr size_t smem_bytes() { return PencilGeom<N, T>::se_offset(THREADS) + sizeof(double) * N; }
 };
 
-// The members of one order only, with that order's register-pencil geometry: its block size,
-// a register cap and one body instantiation per warp (the j chunk a template constant), so each
-// order gets its own register allocation instead of the largest order's.
+// The members of one order only, with the register-pencil tile body: one body instantiation per
+// warp (the j chunk a template constant, so the u coefficients are constant-bank operands) and
+// the order's own register allocation instead of the largest order's.
 template <typename T, int N>
 __global__ void __launch_bounds__(EnsOrderGeom<N, T>::THREADS, EnsOrderGeom<N, T>::MIN_BLOCKS)
 ens_order_kernel(const EnsMember *__restrict__ members, const int *__restrict__ cta_items,
                  const EnsItem *__restrict__ items, int stage) {
-    using GP = PencilGeom<N, T>;
+    using GP = EnsOrderGeom<N, T>;
     __shared__ StageArgs sArgs;
     __shared__ int sActive;
     for (int it = cta_items[blockIdx.x]; it < cta_items[blockIdx.x + 1]; ++it) {
@@ -213,6 +231,11 @@ struct vl_ens {
     };
     bool by_order = false;
     std::vector<Group> groups;
+    // the order groups of one stage run concurrently: group k > 0 on side[k - 1], forked from and
+    // joined back into the caller's stream by events (graph branches when captured)
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> joined;
+    cudaEvent_t forked = nullptr;
     vl::EnsMember *d_members = nullptr;
     vl::FieldArgs *d_field[3] = {nullptr, nullptr, nullptr};
     int *d_cta_items = nullptr;
@@ -273,7 +296,7 @@ int launch_stage(vl_ens *E, int stage, cudaStream_t s) {
 // resident CTAs per SM of one order's kernel (sets its dynamic shared-memory limit first)
 template <typename T, int N>
 int order_blocks(int *blocks) {
-    using GP = vl::PencilGeom<N, T>;
+    using GP = vl::EnsOrderGeom<N, T>;
     VL_ECUDA(cudaFuncSetAttribute(vl::ens_order_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)GP::smem_bytes()));
     VL_ECUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, vl::ens_order_kernel<T, N>, GP::THREADS,
@@ -284,7 +307,7 @@ int order_blocks(int *blocks) {
 
 template <typename T, int N>
 int launch_order(vl_ens *E, const vl_ens::Group &g, int stage, cudaStream_t s) {
-    using GP = vl::PencilGeom<N, T>;
+    using GP = vl::EnsOrderGeom<N, T>;
     vl::ens_order_kernel<T, N><<<g.ctas, GP::THREADS, GP::smem_bytes(), s>>>(E->d_members, E->d_cta_items + g.base,
                                                                               E->d_items, stage);
     const cudaError_t e = cudaGetLastError();
@@ -311,13 +334,27 @@ int with_order(int n, F &&f) {
 
 int stage(vl_ens *E, int st, cudaStream_t s) {
     if (E->by_order) {
-        for (const vl_ens::Group &g : E->groups) {
+        const int ng = (int)E->groups.size();
+        const bool fork = VL_ENS_CONCURRENT && ng > 1;
+        if (fork) {
+            VL_ECUDA(cudaEventRecord(E->forked, s));
+            for (int k = 1; k < ng; ++k) VL_ECUDA(cudaStreamWaitEvent(E->side[k - 1], E->forked, 0));
+        }
+        for (int k = 0; k < ng; ++k) {
+            const vl_ens::Group &g = E->groups[k];
+            cudaStream_t gs = (fork && k > 0) ? E->side[k - 1] : s;
             const int rc = with_order(g.n, [&](auto nc) {
                 constexpr int N = decltype(nc)::value;
-                return E->precision == VL_FP64 ? launch_order<double, N>(E, g, st, s)
-                                               : launch_order<float, N>(E, g, st, s);
+                return E->precision == VL_FP64 ? launch_order<double, N>(E, g, st, gs)
+                                               : launch_order<float, N>(E, g, st, gs);
             });
             if (rc) return rc;
+        }
+        if (fork) {
+            for (int k = 1; k < ng; ++k) {
+                VL_ECUDA(cudaEventRecord(E->joined[k - 1], E->side[k - 1]));
+                VL_ECUDA(cudaStreamWaitEvent(s, E->joined[k - 1], 0));
+            }
         }
         return VL_OK;
     }
@@ -358,10 +395,13 @@ struct CostItem {
     vl::EnsItem it;
 };
 
-// longest processing time first onto the least-loaded of P CTAs; appends the CTAs' item ranges
-// (P + 1 offsets) and items
-void assign_lpt(std::vector<CostItem> &items, int P, std::vector<int> &offs, std::vector<vl::EnsItem> &flat) {
-    std::sort(items.begin(), items.end(), [](const CostItem &a, const CostItem &b) { return a.cost > b.cost; });
+// items in member-major order (members, then x elements, then tile groups), each onto the
+// least-loaded of P CTAs: with items of similar cost this deals them round-robin, so CTAs
+// working at the same time hold neighbouring x elements of one member and the face planes they
+// share are read from L2 (against longest-processing-time order: 64-member FP32 ensemble 2% faster
+// at 4 items per CTA, 11% at 1)
+void assign_in_order(const std::vector<CostItem> &items, int P, std::vector<int> &offs,
+                     std::vector<vl::EnsItem> &flat) {
     std::vector<std::vector<vl::EnsItem>> per(P);
     using Load = std::pair<double, int>;
     std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
@@ -377,6 +417,12 @@ void assign_lpt(std::vector<CostItem> &items, int P, std::vector<int> &offs, std
         flat.insert(flat.end(), per[p].begin(), per[p].end());
     }
     offs.push_back((int)flat.size());
+}
+
+// longest processing time first onto the least-loaded of P CTAs
+void assign_lpt(std::vector<CostItem> &items, int P, std::vector<int> &offs, std::vector<vl::EnsItem> &flat) {
+    std::stable_sort(items.begin(), items.end(), [](const CostItem &a, const CostItem &b) { return a.cost > b.cost; });
+    assign_in_order(items, P, offs, flat);
 }
 
 // rebuild the device descriptors and the item list after a bind or schedule change
@@ -411,7 +457,7 @@ int commit(vl_ens *E) {
             std::vector<CostItem> &list = items[g.n];
             g.ctas = std::max(1, std::min(g.ctas, (int)list.size()));
             g.base = (int)offs.size();
-            assign_lpt(list, g.ctas, offs, flat);
+            assign_in_order(list, g.ctas, offs, flat);
         }
     } else {
         const int P = std::max(1, std::min(E->ctas, (int)items[0].size()));
@@ -501,6 +547,9 @@ VL_API int vl_ens_destroy(vl_ens *E) {
     for (int k = 0; k < 3; ++k) cudaFree(E->d_field[k]);
     cudaFree(E->d_cta_items);
     cudaFree(E->d_items);
+    for (cudaStream_t st : E->side) cudaStreamDestroy(st);
+    for (cudaEvent_t ev : E->joined) cudaEventDestroy(ev);
+    if (E->forked) cudaEventDestroy(E->forked);
     delete E;
     return VL_OK;
 }
@@ -641,6 +690,15 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta) {
         const int tiles = tiles_of(c);
         const int G = (int)(tiles * n * n * n / target + 0.5);
         E->G[i] = std::max(1, std::min(G, tiles));
+    }
+    if (!E->forked) VL_ECUDA(cudaEventCreateWithFlags(&E->forked, cudaEventDisableTiming));
+    while (E->side.size() + 1 < groups.size()) {
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev = nullptr;
+        VL_ECUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        E->side.push_back(st);
+        VL_ECUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        E->joined.push_back(ev);
     }
     E->groups = groups;
     E->by_order = true;

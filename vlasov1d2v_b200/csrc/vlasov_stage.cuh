@@ -26,12 +26,16 @@ namespace vl {
 template <int N, typename T>
 struct PencilGeom {
     static constexpr int EPW = 32 / N;                       // v elements per warp (tile)
-    static constexpr int JC_TARGET = sizeof(T) == 8 ? 2 : 4; // j values per thread
+    // j values per thread: 2 in FP64; in FP32 all rows in one warp up to order 7 and 5 + 4 rows
+    // in two warps at order 9, with the registers uncapped (per combination stage against 4 rows
+    // per thread at 128 registers: order 7 at 32^3 elements 0.082 against 0.090 ms, order 9 at 64^3
+    // 1.62 against 1.635 and its Euler stage 1.47 against 1.60; order 6 unchanged)
+    static constexpr int JC_TARGET = sizeof(T) == 8 ? 2 : (N <= 7 ? N : (N == 9 ? 5 : 4));
     static constexpr int JS = (N + JC_TARGET - 1) / JC_TARGET;
     static constexpr int JC = (N + JS - 1) / JS;
     static constexpr int THREADS = 32 * JS;
     // resident CTAs per SM requested from the compiler (register cap per thread)
-    static constexpr int REG_CAP = VL_STAGE_REG_CAP;
+    static constexpr int REG_CAP = (sizeof(T) == 4 && JC >= 5) ? 255 : VL_STAGE_REG_CAP;
     static constexpr int MIN_BLOCKS = 65536 / (THREADS * REG_CAP) > 0 ? 65536 / (THREADS * REG_CAP) : 1;
     static constexpr int RW = EPW * N;                       // shared row length (v nodes)
     static constexpr int VEC = (sizeof(T) == 8) ? ((N % 2 == 0) ? 2 : 1) : ((N % 4 == 0) ? 4 : 1);
