@@ -47,7 +47,8 @@ def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
         np.testing.assert_allclose(p.stepper.time_array, s.stepper.time_array, rtol=tol)
 
 
-def test_ensemble_final_times_and_autotune(cuda):
+@pytest.mark.parametrize("schedule", [None, (0, 0, 2)], ids=["tuned", "by_order"])
+def test_ensemble_final_times_and_autotune(cuda, schedule):
     from vlasov1d2v_b200.ensemble import Ensemble
 
     probs = [_build(q, "fp64", 8) for q in MEMBERS[:3]]
@@ -67,6 +68,8 @@ def test_ensemble_final_times_and_autotune(cuda):
     assert res["schedule"] in [list(c) for c in cands] and len(res["trials"]) == 4
     for p, f0 in zip(probs, f_before):   # tuning restored the states
         np.testing.assert_array_equal(p.f.arr.get(), f0)
+    if schedule is not None:
+        ens.set_schedule(*schedule)
     ens.run_steps(8)
     assert probs[0].stepper.steps_counter == 8 and probs[2].stepper.steps_counter == 8
     assert 2 <= probs[1].stepper.steps_counter <= 3

@@ -25,7 +25,7 @@ import torch
 from . import _device, _lib
 from .timestep import NonFiniteError, get_max_speeds
 
-DEFAULT_SCHEDULE = (128, 2, 2)
+DEFAULT_SCHEDULE = (0, 0, 8)   # by order, 8 work items per CTA (the autotuner's choice on B200)
 _CACHE = os.path.join(os.path.expanduser("~"), ".cache", "vlasov1d2v_b200", "ensemble_schedules.json")
 
 
