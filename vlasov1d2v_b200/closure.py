@@ -287,17 +287,29 @@ def make_pair(fine, coarse, projector, escale):
 _RK = [(None, None, 1.0), (3.0 / 4.0, 1.0 / 4.0, 1.0 / 4.0), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
 
 
+def runaway(times, energies, start, max_rate):
+    """True when the field energies from index ``start`` on rise above the largest earlier one,
+    W_max at t_max, by more than exp(2 max_rate (t_end - t_max)), t_end the last time."""
+    past = energies[:start]
+    i_max = max(range(len(past)), key=past.__getitem__)
+    w0 = max(past[i_max], 1e-300)
+    span = max(times[-1] - times[i_max], 1e-300)
+    return max(energies[start:]) > w0 * math.exp(2.0 * max_rate * span)
+
+
 class ClosureStepper:
     """Nonlinear SSP-RK3 on a coarse problem with the learned RHS correction after every stage;
     ``mlp=None`` runs the plain coarse operator through the same loop.  One step is a fixed
     sequence of device launches (native kernels + a few torch reductions), CUDA-graph captured."""
 
-    def __init__(self, coarse, mlp=None, escale=1.0):
+    def __init__(self, coarse, mlp=None, escale=1.0, alpha=1.0):
+        """``alpha`` scales the learned correction (1: as trained; below 1: relaxed)."""
         from .context import get_context
 
         self.p = coarse
         self.mlp = mlp
         self.escale = float(escale)
+        self.alpha = float(alpha)
         g = coarse.grids
         self.ctx = get_context(g, precision="fp64", accel=coarse.refs.electron_acceleration_multiplier,
                                bfield=coarse.elliptic.magnetic_field, kappa=coarse.elliptic.poisson_coefficient,
@@ -341,7 +353,8 @@ class ClosureStepper:
                   _vp(self.X), _vp(self.sc), _stream())
         self.mlp.forward(self.X, self.Y)
         _lib.call("vl_closure_apply", _vp(out), _lib.VL_FP64, self.nx, g.u.res, g.v.res, _vp(self.Y),
-                  _vp(self.sc), self.cscale, float(self.mlp.ymax), _vp(self.dt), float(c2), None, _stream())
+                  _vp(self.sc), self.cscale, float(self.mlp.ymax), _vp(self.dt), float(c2 * self.alpha), None,
+                  _stream())
 
     def _step(self, k):
         f, sa, sb = self.f, self.sa, self.sb
@@ -364,9 +377,11 @@ class ClosureStepper:
 
     def run_steps(self, nsteps, batch=32, use_graph=True, max_rate=0.5):
         """Advance ``nsteps`` steps.  Fallback: a batch whose energy or dt is non-finite, or in
-        which the field energy grows faster than exp(2 max_rate t) (far above the physical
-        growth rates of the cyclotron-harmonic instability), is undone and the run continues
-        with the plain coarse operator (``fallback_step`` records where)."""
+        which the field energy rises above its largest earlier value W_max by more than
+        exp(2 max_rate (t - t_max)) (far above the physical growth rates of the cyclotron-harmonic
+        instability; measured from the earlier maximum, not from the batch's first step, because
+        the field energy oscillates through deep minima early in a run), is undone and the run
+        continues with the plain coarse operator (``fallback_step`` records where)."""
         dev = self.f.device
         done = 0
         while done < nsteps:
@@ -378,9 +393,7 @@ class ClosureStepper:
             except FloatingPointError:
                 bad = True
             if not bad and self.mlp is not None:
-                w0 = max(self.energies[snap[3] - 1], 1e-300)
-                dt_b = max(self.time - snap[2], 1e-300)
-                bad = max(self.energies[snap[3]:]) > w0 * math.exp(2.0 * max_rate * dt_b)
+                bad = runaway(self.times, self.energies, snap[3], max_rate)
             if bad:
                 if self.mlp is None:
                     raise FloatingPointError("non-finite energy or dt in the plain coarse run")
@@ -436,4 +449,4 @@ class ClosureStepper:
 
 
 __all__ = ["MLP", "train", "evaluate", "Projector", "projection_1d", "make_pair", "features",
-           "ClosureStepper", "correction_scale"]
+           "ClosureStepper", "correction_scale", "runaway"]
