@@ -260,8 +260,11 @@ VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, i
  *                     per CTA (tile groups per x slab follow from it)
  *   vl_ens_schedule_by_order
  *                     alternative schedule: one stage launch per order present, each kernel
- *                     built for its order alone (block size and register cap of that order's
- *                     register-pencil kernel, as many CTAs as stay resident), work items per CTA
+ *                     built for its order alone (as many CTAs as stay resident, work items per
+ *                     CTA), except for the orders whose bit n is set in native_orders: their
+ *                     members are launched one by one through their own context's stage kernel
+ *                     (the single-problem kernel choice, e.g. the tensor-core one for n = 8);
+ *                     the launches of one stage run on concurrent streams
  *   vl_ens_commit     upload descriptors and the item list (synchronous; not inside a capture)
  *   vl_ens_steps      nsteps SSP-RK3 steps of every member (stream-ordered, capturable)      */
 typedef struct vl_ens vl_ens;
@@ -271,7 +274,7 @@ VL_API size_t vl_ens_workspace_bytes(const vl_ens *ens, int32_t i);
 VL_API int vl_ens_bind(vl_ens *ens, int32_t i, void *f, void *stage_a, void *stage_b, double *E,
                        double *phi, vl_run_state *state, void *workspace);
 VL_API int vl_ens_schedule(vl_ens *ens, int32_t threads, int32_t ctas_per_sm, int32_t items_per_cta);
-VL_API int vl_ens_schedule_by_order(vl_ens *ens, int32_t items_per_cta);
+VL_API int vl_ens_schedule_by_order(vl_ens *ens, int32_t items_per_cta, uint32_t native_orders);
 VL_API int vl_ens_commit(vl_ens *ens);
 VL_API int vl_ens_steps(vl_ens *ens, int32_t nsteps, void *stream);
 

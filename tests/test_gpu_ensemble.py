@@ -23,7 +23,8 @@ def _build(q, precision, batch):
                          background_split=False, **q)
 
 
-@pytest.mark.parametrize("schedule", [None, (0, 0, 2)], ids=["fused", "by_order"])
+@pytest.mark.parametrize("schedule", [(128, 2, 2), (0, 0, 2), (0, 1 << 8, 2), (0, 0x3FE, 2)],
+                         ids=["fused", "by_order", "by_order_native8", "all_native"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
 def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
     from vlasov1d2v_b200.ensemble import Ensemble
@@ -36,8 +37,7 @@ def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
         singles.append(p)
     probs = [_build(q, precision, 3) for q in MEMBERS]
     ens = Ensemble(probs, batch_steps=3)
-    if schedule is not None:
-        ens.set_schedule(*schedule)
+    ens.set_schedule(*schedule)
     ens.run_steps(3)
     ens.run_steps(3, use_graph=False)
     for p, s in zip(probs, singles):
@@ -47,7 +47,7 @@ def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
         np.testing.assert_allclose(p.stepper.time_array, s.stepper.time_array, rtol=tol)
 
 
-@pytest.mark.parametrize("schedule", [None, (0, 0, 2)], ids=["tuned", "by_order"])
+@pytest.mark.parametrize("schedule", [None, (0, 0, 2), (0, 1 << 8, 2)], ids=["tuned", "by_order", "native8"])
 def test_ensemble_final_times_and_autotune(cuda, schedule):
     from vlasov1d2v_b200.ensemble import Ensemble
 

@@ -110,7 +110,7 @@ def _declare(lib):
     lib.vl_ens_workspace_bytes.restype = ctypes.c_size_t
     lib.vl_ens_bind.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp]
     lib.vl_ens_schedule.argtypes = [vp, i32, i32, i32]
-    lib.vl_ens_schedule_by_order.argtypes = [vp, i32]
+    lib.vl_ens_schedule_by_order.argtypes = [vp, i32, ctypes.c_uint32]
     lib.vl_ens_commit.argtypes = [vp]
     lib.vl_ens_steps.argtypes = [vp, i32, vp]
     f32, f64 = ctypes.c_float, ctypes.c_double

@@ -609,6 +609,10 @@ int vl_internal_moment(const vl_ctx *c, const void *f, double *out, int G, cudaS
     return moment(c, f, out, G, s);
 }
 
+vl::StageArgs vl_internal_stage_args(const vl_ctx *c) { return stage_args(c); }
+
+int vl_internal_stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) { return stage(c, a, s); }
+
 extern "C" {
 
 const char *vl_last_error(void) { return g_err.c_str(); }

@@ -50,3 +50,7 @@ struct vl_ctx {
 // helpers of vlasov_api.cu used by the other translation units
 void vl_internal_set_error(const char *msg);
 int vl_internal_moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s);
+// the context's stage arguments (tables, grid, physics) and its single-problem stage launch with
+// the kernel chosen for it; moment partials are written for G = c->stage_grid_g
+vl::StageArgs vl_internal_stage_args(const vl_ctx *c);
+int vl_internal_stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s);

@@ -56,7 +56,7 @@ struct EnsItem {
 };
 
 // RK stage s of the nonlinear SSP-RK3 (main/timestep.py:157-163, :174-182)
-__device__ __forceinline__ void ens_stage_args(StageArgs &a, const EnsMember &m, int s) {
+__host__ __device__ __forceinline__ void ens_stage_args(StageArgs &a, const EnsMember &m, int s) {
     if (s == 0) {
         a.in = m.f;
         a.fn = nullptr;
@@ -228,11 +228,15 @@ struct vl_ens {
     // by-order schedule: one stage launch per order present (ctas CTAs from cta_items[base])
     struct Group {
         int n, ctas, base;
+        bool native;   // members launched one by one through their context's stage kernel
     };
     bool by_order = false;
     std::vector<Group> groups;
-    // the order groups of one stage run concurrently: group k > 0 on side[k - 1], forked from and
-    // joined back into the caller's stream by events (graph branches when captured)
+    // the launches of one by-order stage (one per ordinary group, one per member of a native
+    // group) run concurrently: launch q on lane q mod LANES (lane 0 the caller's stream, lane k > 0
+    // side[k - 1]), the side streams forked from and joined back into the caller's stream by
+    // events (graph branches when captured)
+    static constexpr int LANES = 8;
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> joined;
     cudaEvent_t forked = nullptr;
@@ -332,26 +336,55 @@ int with_order(int n, F &&f) {
     }
 }
 
+// one member's RK stage st through its context's single-problem stage kernel
+int native_stage(vl_ens *E, int i, int st, cudaStream_t s) {
+    vl_ctx *c = E->ctx[i];
+    const vl::EnsMember &m = E->members[i];
+    vl::StageArgs a = vl_internal_stage_args(c);
+    a.E = m.a.E;
+    a.dt = m.a.dt;
+    a.state = m.a.state;
+    a.err = m.a.err;
+    a.partials = m.a.partials;
+    a.xhalo = m.a.xhalo;
+    vl::ens_stage_args(a, m, st);
+    return vl_internal_stage(c, a, s);
+}
+
 int stage(vl_ens *E, int st, cudaStream_t s) {
     if (E->by_order) {
-        const int ng = (int)E->groups.size();
-        const bool fork = VL_ENS_CONCURRENT && ng > 1;
-        if (fork) {
-            VL_ECUDA(cudaEventRecord(E->forked, s));
-            for (int k = 1; k < ng; ++k) VL_ECUDA(cudaStreamWaitEvent(E->side[k - 1], E->forked, 0));
+        // launches of this stage: ordinary groups, then the members of native groups
+        std::vector<std::pair<int, int>> work;   // (group, member or -1)
+        for (int k = 0; k < (int)E->groups.size(); ++k) {
+            if (!E->groups[k].native) {
+                work.push_back({k, -1});
+            } else {
+                for (int i = 0; i < (int)E->ctx.size(); ++i)
+                    if (E->ctx[i]->cfg.n == E->groups[k].n) work.push_back({k, i});
+            }
         }
-        for (int k = 0; k < ng; ++k) {
-            const vl_ens::Group &g = E->groups[k];
-            cudaStream_t gs = (fork && k > 0) ? E->side[k - 1] : s;
-            const int rc = with_order(g.n, [&](auto nc) {
-                constexpr int N = decltype(nc)::value;
-                return E->precision == VL_FP64 ? launch_order<double, N>(E, g, st, gs)
-                                               : launch_order<float, N>(E, g, st, gs);
-            });
+        const int lanes = VL_ENS_CONCURRENT ? std::min<int>(vl_ens::LANES, (int)work.size()) : 1;
+        if (lanes > 1) {
+            VL_ECUDA(cudaEventRecord(E->forked, s));
+            for (int k = 1; k < lanes; ++k) VL_ECUDA(cudaStreamWaitEvent(E->side[k - 1], E->forked, 0));
+        }
+        for (int q = 0; q < (int)work.size(); ++q) {
+            const vl_ens::Group &g = E->groups[work[q].first];
+            cudaStream_t ls = (q % lanes == 0) ? s : E->side[q % lanes - 1];
+            int rc;
+            if (work[q].second >= 0) {
+                rc = native_stage(E, work[q].second, st, ls);
+            } else {
+                rc = with_order(g.n, [&](auto nc) {
+                    constexpr int N = decltype(nc)::value;
+                    return E->precision == VL_FP64 ? launch_order<double, N>(E, g, st, ls)
+                                                   : launch_order<float, N>(E, g, st, ls);
+                });
+            }
             if (rc) return rc;
         }
-        if (fork) {
-            for (int k = 1; k < ng; ++k) {
+        if (lanes > 1) {
+            for (int k = 1; k < lanes; ++k) {
                 VL_ECUDA(cudaEventRecord(E->joined[k - 1], E->side[k - 1]));
                 VL_ECUDA(cudaStreamWaitEvent(s, E->joined[k - 1], 0));
             }
@@ -454,6 +487,7 @@ int commit(vl_ens *E) {
     std::vector<vl::EnsItem> flat;
     if (E->by_order) {
         for (vl_ens::Group &g : E->groups) {
+            if (g.native) continue;
             std::vector<CostItem> &list = items[g.n];
             g.ctas = std::max(1, std::min(g.ctas, (int)list.size()));
             g.base = (int)offs.size();
@@ -464,6 +498,7 @@ int commit(vl_ens *E) {
         E->ctas = P;
         assign_lpt(items[0], P, offs, flat);
     }
+    if (offs.empty()) offs.push_back(0);   // every group native: no work list
     cudaFree(E->d_cta_items);
     cudaFree(E->d_items);
     E->d_cta_items = nullptr;
@@ -657,7 +692,7 @@ VL_API int vl_ens_schedule(vl_ens *E, int32_t threads, int32_t ctas_per_sm, int3
     return VL_OK;
 }
 
-VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta) {
+VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta, uint32_t native_orders) {
     if (!E) return efail(VL_ERR_INVALID, "null ensemble");
     if (items_per_cta < 1 || items_per_cta > 64) return efail(VL_ERR_INVALID, "items_per_cta in 1..64");
     const int count = (int)E->ctx.size();
@@ -667,32 +702,50 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta) {
         const double n = c->cfg.n;
         total[c->cfg.n] += (double)c->cfg.nx * tiles_of(c) * n * n * n;
     }
-    // one group per order present, as many CTAs as its kernel keeps resident on the device
+    // one group per order present: native (members through their own contexts' stage kernels)
+    // or as many CTAs of the order's ensemble kernel as it keeps resident on the device
     std::vector<vl_ens::Group> groups;
+    int launches = 0;
     for (int n = vl::NMAX; n >= 1; --n) {
         if (total[n] == 0.0) continue;
+        if ((native_orders >> n) & 1u) {
+            groups.push_back({n, 0, 0, true});
+            for (int i = 0; i < count; ++i) launches += (E->ctx[i]->cfg.n == n);
+            continue;
+        }
         int blocks = 0;
         const int rc = with_order(n, [&](auto nc) {
             constexpr int N = decltype(nc)::value;
             return E->precision == VL_FP64 ? order_blocks<double, N>(&blocks) : order_blocks<float, N>(&blocks);
         });
         if (rc) return rc;
-        groups.push_back({n, E->sm_count * blocks, 0});
+        groups.push_back({n, E->sm_count * blocks, 0, false});
+        ++launches;
     }
-    // tile groups per member: about items_per_cta items of similar cost per CTA of its order
+    // tile groups per member: its context's own for native groups (the partials layout of the
+    // single-problem kernel), else about items_per_cta items of similar cost per CTA of its order
     for (int i = 0; i < count; ++i) {
         const vl_ctx *c = E->ctx[i];
         const double n = c->cfg.n;
         int ctas = 1;
+        bool native = false;
         for (const vl_ens::Group &g : groups)
-            if (g.n == c->cfg.n) ctas = g.ctas;
+            if (g.n == c->cfg.n) {
+                ctas = g.ctas;
+                native = g.native;
+            }
+        if (native) {
+            E->G[i] = c->stage_grid_g;
+            continue;
+        }
         const double target = total[c->cfg.n] / ((double)ctas * items_per_cta);
         const int tiles = tiles_of(c);
         const int G = (int)(tiles * n * n * n / target + 0.5);
         E->G[i] = std::max(1, std::min(G, tiles));
     }
     if (!E->forked) VL_ECUDA(cudaEventCreateWithFlags(&E->forked, cudaEventDisableTiming));
-    while (E->side.size() + 1 < groups.size()) {
+    const int lanes = std::min(vl_ens::LANES, std::max(launches, 1));
+    while ((int)E->side.size() + 1 < lanes) {
         cudaStream_t st = nullptr;
         cudaEvent_t ev = nullptr;
         VL_ECUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));

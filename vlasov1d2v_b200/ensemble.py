@@ -9,8 +9,10 @@ Each member keeps its own loop state, so members with different final times shar
 ``autotune`` picks the driver's schedule -- threads per CTA, resident CTAs per SM and work
 items per CTA -- by timing candidate schedules on the ensemble itself (states restored
 afterwards), and caches the winner per ensemble signature and GPU in a JSON file.  A schedule
-``(0, 0, items_per_cta)`` is the by-order form: one stage launch per order present, each kernel
-compiled for its order alone (``vl_ens_schedule_by_order``).
+``(0, native, items_per_cta)`` is the by-order form (``vl_ens_schedule_by_order``): one stage
+launch per order present, each kernel compiled for its order alone, except for the orders whose
+bit n is set in ``native``, whose members run one by one through their own single-problem stage
+kernel (the tensor-core kernel for n = 8); the launches of a stage run on concurrent streams.
 """
 from __future__ import annotations
 
@@ -78,9 +80,10 @@ class Ensemble:
     # -- schedule --------------------------------------------------------------------------------
     def set_schedule(self, threads, ctas_per_sm, items_per_cta):
         """threads 64 or 128 with ``ctas_per_sm`` resident CTAs: one stage kernel for all orders;
-        threads 0: the by-order form (block size and residency of each order's own kernel)."""
+        threads 0: the by-order form, ``ctas_per_sm`` then the bit mask of the orders run through
+        their members' own single-problem stage kernels."""
         if int(threads) == 0:
-            _lib.call("vl_ens_schedule_by_order", self.handle, int(items_per_cta))
+            _lib.call("vl_ens_schedule_by_order", self.handle, int(items_per_cta), int(ctas_per_sm))
         else:
             _lib.call("vl_ens_schedule", self.handle, int(threads), int(ctas_per_sm), int(items_per_cta))
         _lib.call("vl_ens_commit", self.handle)
@@ -133,7 +136,8 @@ class Ensemble:
         if candidates is None:
             candidates = [(t, c, k) for t in (128, 64) for c in (1, 2, 3, 4) for k in (1, 2, 4, 8)
                           if not (t == 128 and c > 2)]
-            candidates += [(0, 0, k) for k in (1, 2, 4, 8)]
+            candidates += [(0, native, k) for native in (0, 1 << 8) for k in (1, 2, 4, 8)]
+            candidates += [(0, 0x3FE, 8)]   # every order through the single-problem kernels
         snap = self._snapshot()
         trials = []
         try:
