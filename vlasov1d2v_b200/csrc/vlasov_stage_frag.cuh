@@ -51,6 +51,11 @@
 #ifndef VL_FRAG_JS64
 #define VL_FRAG_JS64 1
 #endif
+// stage buffers released per warp on an "empty" barrier that the issuing thread waits on (1),
+// or by a CTA-wide barrier after each tile (0)
+#ifndef VL_FRAG_EMPTYBAR
+#define VL_FRAG_EMPTYBAR 0
+#endif
 #ifndef VL_FRAG_JS32
 #define VL_FRAG_JS32 1
 #endif
@@ -166,6 +171,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     __shared__ __align__(8) uint64_t full[2];
+    __shared__ __align__(8) uint64_t empty[2];   // VL_FRAG_EMPTYBAR: one arrival per warp and tile
     __shared__ dd sRed[EPT * G::JS][N];
 
     const int tid = threadIdx.x;
@@ -203,6 +209,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
+        mbar_init(&empty[0], NT / 32);
+        mbar_init(&empty[1], NT / 32);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -492,9 +500,26 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     rows(std::integral_constant<int, G::NJ>{});
             }
         }
+#if VL_FRAG_EMPTYBAR
+        // this warp is done with stage s; the issuing thread waits for every warp (use q >> 1 of
+        // the barrier) before refilling it, the other warps go on to the next tile
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
+        if (tid == 0 && q + 2 < ntile_cta) {
+            if (!mbar_wait_bounded(&empty[s], (uint32_t)((q >> 1) & 1))) {
+                if (a.err != nullptr) atomicOr(a.err, 2);
+                return;
+            }
+            issue(s, q + 2);
+        }
+#else
         __syncthreads();   // stage s fully consumed
         if (tid == 0 && q + 2 < ntile_cta) issue(s, q + 2);
+#endif
     }
+#if VL_FRAG_EMPTYBAR
+    __syncthreads();   // every warp is out of the tile loop before the shared reduction
+#endif
 
     if (a.partials == nullptr) return;
     // moment partial of x node g: sum over the thread's columns, the quad, the warps
