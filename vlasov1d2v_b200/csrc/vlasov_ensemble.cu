@@ -2,17 +2,22 @@
 // physics) advanced by one set of launches per RK stage.
 //
 // Each member is an ordinary vl_ctx with its own state buffers and loop state.  Per RK stage the
-// ensemble issues three launches for all members together: the forward DFT of every member's
-// field solve, the inverse DFT (+ loop bookkeeping), and one persistent stage kernel whose CTAs
-// walk a precomputed list of work items (member, x element, tile group).  The item list is built
-// on the host by longest-processing-time-first assignment of estimated costs to CTAs, so members
-// of very different sizes share the device evenly.  The CTA count, block size and items per CTA
-// are the schedule's tunables (chosen by the autotuner in vlasov1d2v_b200/ensemble.py).
+// ensemble issues the forward DFT of every member's field solve and the inverse DFT (+ loop
+// bookkeeping) as one launch each, then the stage work in one of two forms:
+//   fused     one persistent kernel whose CTAs walk a precomputed list of work items (member,
+//             x element, tile group), built on the host by longest-processing-time-first
+//             assignment of estimated costs; block size, CTAs per SM and items per CTA are the
+//             schedule's tunables;
+//   by order  one persistent kernel per order present, compiled for that order alone, over its
+//             own item list (member-major, least-loaded CTA first); orders marked native instead
+//             launch each member through its own context's single-problem stage kernel; all
+//             launches of a stage run on concurrent streams forked from the caller's.
+// The autotuner in vlasov1d2v_b200/ensemble.py picks among them.
 //
-// The stage work of a member runs through the register-pencil tile body (orders 1..9) with
-// the order-specific up / xi tables in constant memory; the member's velocity weights and scalars
-// come from its descriptor.  Members whose loop state is inactive (final time reached) are
-// skipped by every kernel, so a batch of K steps is correct for members of any final time.
+// The ensemble kernels run the register-pencil tile body (orders 1..9) with the order-specific
+// up / xi tables in constant memory; the member's velocity weights and scalars come from its
+// descriptor.  Members whose loop state is inactive (final time reached) are skipped by every
+// kernel, so a batch of K steps is correct for members of any final time.
 #include <cuda_runtime.h>
 
 #include <algorithm>
