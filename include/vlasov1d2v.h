@@ -248,9 +248,9 @@ VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, i
 /* ---- batched heterogeneous ensemble ------------------------------------------------------------
  * No counterpart in the reference (which runs one problem per process).  Many independent
  * problems -- each an ordinary context of any order 1..9 and grid, one common precision --
- * advance together: per RK stage one forward-DFT launch, one inverse-DFT launch and one
- * persistent stage kernel for all members, the stage kernel's CTAs walking a host-built list of
- * (member, x element, tile group) work items balanced by estimated cost.  Members keep their own
+ * advance together: per RK stage one forward-DFT launch, one inverse-DFT launch and persistent
+ * stage kernels (one for all members, or one per order present) whose CTAs walk host-built lists
+ * of (member, x element, tile group) work items balanced by estimated cost.  Members keep their own
  * loop state (final time, histories); inactive members are skipped on the device.
  *   vl_ens_create     members = existing contexts (borrowed; keep them alive)
  *   vl_ens_bind       member i's state f, stage buffers, E, phi, loop state and workspace of
