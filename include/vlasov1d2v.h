@@ -264,10 +264,12 @@ VL_API int vl_interpolate(const void *f, int32_t prec, int32_t nx, int32_t nu, i
  *                     CTA), except for the orders whose bit n is set in native_orders: their
  *                     members are launched one by one through their own context's stage kernel
  *                     (the single-problem kernel choice, e.g. the tensor-core one for n = 8);
- *                     the launches of one stage run on concurrent streams
+ *                     VL_ENS_NATIVE_AUTO picks the members whose contexts stage their tiles by
+ *                     TMA; the launches of one stage run on concurrent streams
  *   vl_ens_commit     upload descriptors and the item list (synchronous; not inside a capture)
  *   vl_ens_steps      nsteps SSP-RK3 steps of every member (stream-ordered, capturable)      */
 typedef struct vl_ens vl_ens;
+#define VL_ENS_NATIVE_AUTO 0xFFFFFFFFu
 VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out);
 VL_API int vl_ens_destroy(vl_ens *ens);
 VL_API size_t vl_ens_workspace_bytes(const vl_ens *ens, int32_t i);

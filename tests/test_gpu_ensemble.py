@@ -23,8 +23,8 @@ def _build(q, precision, batch):
                          background_split=False, **q)
 
 
-@pytest.mark.parametrize("schedule", [(128, 2, 2), (0, 0, 2), (0, 1 << 8, 2), (0, 0x3FE, 2)],
-                         ids=["fused", "by_order", "by_order_native8", "all_native"])
+@pytest.mark.parametrize("schedule", [(128, 2, 2), (0, 0, 2), (0, 1 << 8, 2), (0, 0x3FE, 2), (0, 0xFFFFFFFF, 2)],
+                         ids=["fused", "by_order", "by_order_native8", "all_native", "native_auto"])
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-5)])
 def test_ensemble_members_match_single_runs(cuda, precision, tol, schedule):
     from vlasov1d2v_b200.ensemble import Ensemble

@@ -44,3 +44,27 @@ def test_fp32_background_split_against_fp64(cuda):
     assert ferr_split < 3e-6
     # the split removes the FP32 cancellation of the background in the x derivative
     assert ferr_split < ferr_plain / 4
+
+
+@pytest.mark.parametrize("split", [True, False], ids=["background_split", "plain_fp32"])
+def test_fp32_generic_tma_form_in_the_loop(cuda, split, monkeypatch):
+    """FP32 order 6 on 16-byte rows, where the generic kernel's TMA form is the stage kernel:
+    without the background split the loop's stages run on it, with the split they go to the
+    register-pencil kernel on its own grid.  Either way 6 steps match a run on the register-pencil
+    kernel alone (VLASOV1D2V_STAGE_KERNEL=pencil)."""
+    from vlasov1d2v_b200 import problem
+
+    def run(tma):
+        if tma:
+            monkeypatch.delenv("VLASOV1D2V_STAGE_KERNEL", raising=False)
+        else:
+            monkeypatch.setenv("VLASOV1D2V_STAGE_KERNEL", "pencil")
+        p = problem.build((4, 4, 6), 6, perturbation="cos", amp=0.01, batch_steps=3, precision="fp32",
+                          background_split=split)
+        p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, 6)
+        return np.asarray(p.stepper.field_energy), p.f.full_array().get()
+
+    w0, f0 = run(False)
+    w1, f1 = run(True)
+    assert rel_err(f1, f0) < 1e-5
+    assert history_err(w1, w0) < 1e-4

@@ -186,22 +186,27 @@ def test_odd_orders_on_aligned_rows(cuda, n):
         assert rel_err(_np(out)[INNER], want[INNER]) < 1e-14
 
 
-@pytest.mark.parametrize("form", ["pencil", "phased"])
-@pytest.mark.parametrize("res", [(2, 2, 3), (2, 2, 4)])
+@pytest.mark.parametrize("form", ["pencil", "phased", "tma"])
+@pytest.mark.parametrize("res", [(2, 2, 3), (2, 2, 4), (2, 2, 2), (2, 3, 6)])
 @pytest.mark.parametrize("n", [3, 5, 6, 7, 9])
 def test_fp32_stage_kernels_other_orders(cuda, n, res, form, monkeypatch):
-    """FP32 orders other than 4 and 8: the register-pencil kernel (the default there) and the
-    generic kernel's phased form, for rows that are not 16-byte multiples ((nv + 2) n floats) but
-    whose rows of one j share a 16-byte phase ((nu + 2) n (nv + 2) n a multiple of 4).  The three
-    RK stage kinds of a random state against the FP64 oracle, within FP32 rounding of the stage
-    results.  The phased form is opt-in (VLASOV1D2V_GEN_PH=1, read when the context is created)."""
+    """FP32 orders other than 4 and 8: the generic kernel's TMA form (the default where the rows
+    are 16-byte multiples, (nv + 2) n a multiple of 4; the register-pencil kernel elsewhere), the
+    register-pencil kernel everywhere (VLASOV1D2V_STAGE_KERNEL=pencil) and the generic kernel's
+    phased form (opt-in VLASOV1D2V_GEN_PH=1 with the TMA form off: rows whose j rows share a
+    16-byte phase, (nu + 2) n (nv + 2) n a multiple of 4).  The three RK stage kinds of a random
+    state against the FP64 oracle, within FP32 rounding of the stage results.  The switches are
+    read when the context is created."""
     from vlasov1d2v_b200 import _lib, problem
     from vlasov1d2v_b200.context import get_context
 
+    for var in ("VLASOV1D2V_GEN_PH", "VLASOV1D2V_GEN_NO_TMA", "VLASOV1D2V_STAGE_KERNEL"):
+        monkeypatch.delenv(var, raising=False)
     if form == "phased":
         monkeypatch.setenv("VLASOV1D2V_GEN_PH", "1")
-    else:
-        monkeypatch.delenv("VLASOV1D2V_GEN_PH", raising=False)
+        monkeypatch.setenv("VLASOV1D2V_GEN_NO_TMA", "1")
+    elif form == "pencil":
+        monkeypatch.setenv("VLASOV1D2V_STAGE_KERNEL", "pencil")
     p = problem.build(res, n, perturbation=None, amp=0.0, precision="fp32")
     c = vo.make_case(*res, n)
     ctx = get_context(p.grids, precision="fp32", accel=p.refs.electron_acceleration_multiplier,

@@ -31,6 +31,7 @@ EXPORTED = (
     "vl_poisson_dg", "vl_axpby_interior",
 )
 NOALLOC_SCRATCH_BYTES = 1 << 20
+VL_ENS_NATIVE_AUTO = 0xFFFFFFFF
 
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
 

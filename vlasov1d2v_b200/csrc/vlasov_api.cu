@@ -172,11 +172,11 @@ int bg_map(vl_ctx *c, const float *ptr, int n, CUtensorMap *out) {
     return VL_OK;
 }
 
-// 5-D view of an FP64 state for the generic kernel's TMA form: which 0 = tile (WB, RJ, 1, n, 1),
+// 5-D view of a state for the generic kernel's TMA form: which 0 = tile (WB, RJ, 1, n, 1),
 // 1 = x-node plane (WB, n, 1, 1, 1), 2 = j row of every x node (WB, 1, 1, n, 1)
-template <int N>
+template <int N, typename T>
 int gen_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
-    using G = vl::GenTmaGeom<N, double>;
+    using G = vl::GenTmaGeom<N, T>;
     auto key = std::make_pair(ptr, 20 + which);
     auto it = c->maps.find(key);
     if (it != c->maps.end()) {
@@ -185,7 +185,7 @@ int gen_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     }
     auto enc = encode_fn();
     if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2, X = c->cfg.nx + 2, es = sizeof(double);
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2, X = c->cfg.nx + 2, es = sizeof(T);
     cuuint64_t dims[5] = {V * N, (cuuint64_t)N, U, (cuuint64_t)N, X};
     cuuint64_t strides[4] = {V * N * es, V * N * N * es, V * N * N * U * es, V * N * N * U * N * es};
     cuuint32_t box[5] = {(cuuint32_t)G::WB, 1, 1, 1, 1};
@@ -199,8 +199,9 @@ int gen_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     }
     cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     CUtensorMap m;
-    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<void *>(ptr), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    CUresult r = enc(&m, sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 5,
+                     const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (generic kernel) failed");
     if (c->maps.size() > 64) c->maps.clear();
@@ -230,7 +231,11 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
         }
     vl::StageArgs a = a0;
     if (a.err == nullptr) a.err = c->d_err;
-    dim3 grid(c->stage_grid_g, c->cfg.nx);
+    // FP32 with the background split has no TMA form of the generic kernel: the register-pencil
+    // kernel takes those launches, on its own grid
+    const bool gen_tma_now = c->stage_kernel == VL_STAGE_GEN && c->gen_tma && (sizeof(T) == 8 || a.bg_rb == nullptr);
+    const bool bg_fallback = c->stage_kernel == VL_STAGE_GEN && c->gen_tma && !gen_tma_now;
+    dim3 grid(bg_fallback ? c->stage_grid_g_bg : c->stage_grid_g, c->cfg.nx);
     if constexpr (N == 8) {
         if (c->use_frag) {
             using G = vl::FragGeom<T>;
@@ -252,20 +257,26 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                                 "stage_frag_kernel");
         }
     }
-    if constexpr (sizeof(T) == 8) {
-        if (c->stage_kernel == VL_STAGE_GEN && c->gen_tma) {
-            using G = vl::GenTmaGeom<N, double>;
+    if (bg_fallback) {
+        using G = vl::PencilGeom<N, T>;
+        return check_launch(launch(c, vl::stage_pencil_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
+                                   tb),
+                            "stage_pencil_kernel");
+    }
+    {
+        if (gen_tma_now) {
+            using G = vl::GenTmaGeom<N, T>;
             if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
                  reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out)) % 16)
                 return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
             vl::GenMaps maps;
             int rc;
-            if ((rc = gen_map<N>(c, a.in, 0, &maps.in_tile))) return rc;
-            if ((rc = gen_map<N>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
-            if ((rc = gen_map<N>(c, a.in, 1, &maps.xface))) return rc;
-            if ((rc = gen_map<N>(c, a.in, 2, &maps.uface))) return rc;
-            return check_launch(launch(c, vl::stage_gen_tma_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s,
-                                       a, tb, maps),
+            if ((rc = gen_map<N, T>(c, a.in, 0, &maps.in_tile))) return rc;
+            if ((rc = gen_map<N, T>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
+            if ((rc = gen_map<N, T>(c, a.in, 1, &maps.xface))) return rc;
+            if ((rc = gen_map<N, T>(c, a.in, 2, &maps.uface))) return rc;
+            return check_launch(launch(c, vl::stage_gen_tma_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(),
+                                       s, a, tb, maps),
                                 "stage_gen_tma_kernel");
         }
     }
@@ -333,10 +344,10 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
+int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool ph) {
     int blocks = 0;
     if constexpr (sizeof(T) == 4) {
-        if (gen && gtma) {   // FP32: the phased form
+        if (gen && ph) {   // FP32: the phased form
             using G = vl::GenPhGeom<N, float>;
             const size_t smem = G::smem_bytes();
             cudaFuncSetAttribute(vl::stage_gen_ph_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -346,16 +357,14 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
             return blocks > 0 ? blocks : 1;
         }
     }
-    if constexpr (sizeof(T) == 8) {
-        if (gen && gtma) {
-            using G = vl::GenTmaGeom<N, double>;
-            const size_t smem = G::smem_bytes();
-            cudaFuncSetAttribute(vl::stage_gen_tma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_tma_kernel<N>, G::THREADS,
-                                                              smem) != cudaSuccess)
-                return 1;
-            return blocks > 0 ? blocks : 1;
-        }
+    if (gen && gtma) {
+        using G = vl::GenTmaGeom<N, T>;
+        const size_t smem = G::smem_bytes();
+        cudaFuncSetAttribute(vl::stage_gen_tma_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_tma_kernel<N, T>, G::THREADS,
+                                                          smem) != cudaSuccess)
+            return 1;
+        return blocks > 0 ? blocks : 1;
     }
     if (gen) {
         using G = vl::GenGeom<N, T>;
@@ -409,18 +418,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma, bool ph) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma);
-        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma);
-        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma);
-        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma);
-        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma);
-        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma);
-        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma);
-        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma);
-        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma);
-        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma, ph);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma, ph);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma, ph);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma, ph);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma, ph);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma, ph);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma, ph);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma, ph);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma, ph);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma, ph);
         default: return 1;
     }
 }
@@ -543,7 +552,8 @@ int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
 
 // byte offset of the field scratch inside a loop workspace (after the moment partials)
 size_t partials_bytes(const vl_ctx *c) {
-    const int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
+    int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
+    if (c->stage_grid_g_bg > g) g = c->stage_grid_g_bg;
     const size_t b = sizeof(double) * (size_t)c->cfg.nx * g * c->cfg.n;
     return (b + 255) & ~(size_t)255;
 }
@@ -738,10 +748,19 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         const char *env = getenv("VLASOV1D2V_GEN_PH");
         c->gen_ph = cfg->precision == VL_FP32 && ph_ok && env && env[0] == '1';
     }
+    // FP32 on the generic kernel's TMA form where the rows are 16-byte multiples ((nv+2) n a
+    // multiple of 4), orders other than 4 and 8 (launches with the background split go to the
+    // register-pencil kernel); VLASOV1D2V_GEN_NO_TMA=1 switches the TMA form off
+    const bool no_gen_tma = [] {
+        const char *env = getenv("VLASOV1D2V_GEN_NO_TMA");
+        return env && env[0] == '1';
+    }();
+    const bool gen_tma32 = cfg->precision == VL_FP32 && ((size_t)(cfg->nv + 2) * n) % 4 == 0 && !no_gen_tma &&
+                           encode_fn() != nullptr;
     c->stage_kernel = c->use_frag                    ? VL_STAGE_FRAG
                       : cfg->precision == VL_FP64    ? VL_STAGE_GEN
                       : c->use_tma                   ? VL_STAGE_TMA
-                      : c->gen_ph                    ? VL_STAGE_GEN
+                      : (c->gen_ph || gen_tma32)     ? VL_STAGE_GEN
                                                      : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
@@ -756,16 +775,13 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         if (c->stage_kernel != VL_STAGE_TMA && c->stage_kernel != VL_STAGE_FRAG) c->use_tma = false;
     }
     const bool gen = c->stage_kernel == VL_STAGE_GEN;
-    // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even)
-    {
-        const char *env = getenv("VLASOV1D2V_GEN_NO_TMA");
-        c->gen_tma = gen && cfg->precision == VL_FP64 && ((size_t)(cfg->nv + 2) * n) % 2 == 0 &&
-                     encode_fn() != nullptr && !(env && env[0] == '1');
-    }
-    c->gen_ph = c->gen_ph && gen;
+    // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even), FP32 as above
+    c->gen_tma = gen && (cfg->precision == VL_FP64 ? ((size_t)(cfg->nv + 2) * n) % 2 == 0 : gen_tma32) &&
+                 encode_fn() != nullptr && !no_gen_tma;
+    c->gen_ph = c->gen_ph && gen && !c->gen_tma;
     const int occ = cfg->precision == VL_FP64
-                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma)
-                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_ph);
+                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma, false)
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma, c->gen_ph);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double
@@ -774,6 +790,16 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if (g > tiles) g = tiles;
     if (g < 1) g = 1;
     c->stage_grid_g = g;
+    c->stage_grid_g_bg = g;
+    if (cfg->precision == VL_FP32 && c->gen_tma) {   // the register-pencil kernel's own grid
+        const int occ_p = stage_occupancy<float>(n, false, false, false, false, false);
+        const int bp = 32 / n > 0 ? 32 / n : 1;
+        const int tiles_p = cfg->nu * ((cfg->nv + bp - 1) / bp);
+        int gp = (c->sm_count * occ_p) / cfg->nx;
+        if (gp > tiles_p) gp = tiles_p;
+        if (gp < 1) gp = 1;
+        c->stage_grid_g_bg = gp;
+    }
     // standalone moment: MOMENT_CTAS_PER_SM resident CTAs per SM, at most one per u element
     int gm = (c->sm_count * vl::MOMENT_CTAS_PER_SM) / cfg->nx;
     if (gm > cfg->nu) gm = cfg->nu;
@@ -958,7 +984,9 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     cudaStream_t s = as_stream(stream);
     double *partials = static_cast<double *>(workspace);
     double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) + partials_bytes(c));
-    const int G = c->stage_grid_g;
+    // FP32 with the background split on a generic-TMA context: the register-pencil kernel's grid
+    const int G = (c->cfg.precision == VL_FP32 && c->gen_tma && c->bg_rb != nullptr) ? c->stage_grid_g_bg
+                                                                                       : c->stage_grid_g;
     int rc;
     // the field solve's ticket counter starts at zero (the last CTA of each record resets it)
     VL_CUDA(cudaMemsetAsync(fscratch + 4 * (size_t)c->cfg.n_modes, 0, sizeof(int), s));

@@ -237,6 +237,7 @@ struct vl_ens {
     };
     bool by_order = false;
     std::vector<Group> groups;
+    std::vector<char> native;   // by order: member i launched through its own context
     // the launches of one by-order stage (one per ordinary group, one per member of a native
     // group) run concurrently: launch q on lane q mod LANES (lane 0 the caller's stream, lane k > 0
     // side[k - 1]), the side streams forked from and joined back into the caller's stream by
@@ -365,7 +366,7 @@ int stage(vl_ens *E, int st, cudaStream_t s) {
                 work.push_back({k, -1});
             } else {
                 for (int i = 0; i < (int)E->ctx.size(); ++i)
-                    if (E->ctx[i]->cfg.n == E->groups[k].n) work.push_back({k, i});
+                    if (E->native[i] && E->ctx[i]->cfg.n == E->groups[k].n) work.push_back({k, i});
             }
         }
         const int lanes = VL_ENS_CONCURRENT ? std::min<int>(vl_ens::LANES, (int)work.size()) : 1;
@@ -477,7 +478,8 @@ int commit(vl_ens *E) {
         const int G = E->G[i];
         const double n = c->cfg.n;
         const int tiles = tiles_of(c);
-        std::vector<CostItem> &list = items[E->by_order ? c->cfg.n : 0];
+        // by order: members launched through their own contexts have no items
+        std::vector<CostItem> &list = items[E->by_order ? (E->native[i] ? 0 : c->cfg.n) : 0];
         for (int e = 0; e < c->cfg.nx; ++e)
             for (int g = 0; g < G; ++g) {
                 const int nt = (tiles - g + G - 1) / G;
@@ -701,23 +703,38 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta, uint32_t n
     if (!E) return efail(VL_ERR_INVALID, "null ensemble");
     if (items_per_cta < 1 || items_per_cta > 64) return efail(VL_ERR_INVALID, "items_per_cta in 1..64");
     const int count = (int)E->ctx.size();
+    // members launched through their own contexts: those of the orders in the mask, or with
+    // VL_ENS_NATIVE_AUTO those whose context stages its tiles by TMA (fragment kernel, TMA
+    // kernel, the generic kernel's TMA form), which beat the ensemble's register-pencil body
+    std::vector<char> native(count, 0);
+    for (int i = 0; i < count; ++i) {
+        const vl_ctx *c = E->ctx[i];
+        if (native_orders == VL_ENS_NATIVE_AUTO)
+            native[i] = c->stage_kernel == VL_STAGE_FRAG || c->stage_kernel == VL_STAGE_TMA ||
+                        (c->stage_kernel == VL_STAGE_GEN && c->gen_tma);
+        else
+            native[i] = (native_orders >> c->cfg.n) & 1u;
+    }
     double total[vl::NMAX + 1] = {};
+    bool any_native[vl::NMAX + 1] = {};
     for (int i = 0; i < count; ++i) {
         const vl_ctx *c = E->ctx[i];
         const double n = c->cfg.n;
-        total[c->cfg.n] += (double)c->cfg.nx * tiles_of(c) * n * n * n;
+        if (native[i])
+            any_native[c->cfg.n] = true;
+        else
+            total[c->cfg.n] += (double)c->cfg.nx * tiles_of(c) * n * n * n;
     }
-    // one group per order present: native (members through their own contexts' stage kernels)
-    // or as many CTAs of the order's ensemble kernel as it keeps resident on the device
+    // per order present: a native group (its members one launch each) and / or an ensemble
+    // group (as many CTAs of the order's ensemble kernel as it keeps resident)
     std::vector<vl_ens::Group> groups;
     int launches = 0;
     for (int n = vl::NMAX; n >= 1; --n) {
-        if (total[n] == 0.0) continue;
-        if ((native_orders >> n) & 1u) {
+        if (any_native[n]) {
             groups.push_back({n, 0, 0, true});
-            for (int i = 0; i < count; ++i) launches += (E->ctx[i]->cfg.n == n);
-            continue;
+            for (int i = 0; i < count; ++i) launches += (native[i] && E->ctx[i]->cfg.n == n);
         }
+        if (total[n] == 0.0) continue;
         int blocks = 0;
         const int rc = with_order(n, [&](auto nc) {
             constexpr int N = decltype(nc)::value;
@@ -727,22 +744,18 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta, uint32_t n
         groups.push_back({n, E->sm_count * blocks, 0, false});
         ++launches;
     }
-    // tile groups per member: its context's own for native groups (the partials layout of the
+    // tile groups per member: its context's own for native members (the partials layout of the
     // single-problem kernel), else about items_per_cta items of similar cost per CTA of its order
     for (int i = 0; i < count; ++i) {
         const vl_ctx *c = E->ctx[i];
-        const double n = c->cfg.n;
-        int ctas = 1;
-        bool native = false;
-        for (const vl_ens::Group &g : groups)
-            if (g.n == c->cfg.n) {
-                ctas = g.ctas;
-                native = g.native;
-            }
-        if (native) {
+        if (native[i]) {
             E->G[i] = c->stage_grid_g;
             continue;
         }
+        const double n = c->cfg.n;
+        int ctas = 1;
+        for (const vl_ens::Group &g : groups)
+            if (g.n == c->cfg.n && !g.native) ctas = g.ctas;
         const double target = total[c->cfg.n] / ((double)ctas * items_per_cta);
         const int tiles = tiles_of(c);
         const int G = (int)(tiles * n * n * n / target + 0.5);
@@ -759,6 +772,7 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta, uint32_t n
         E->joined.push_back(ev);
     }
     E->groups = groups;
+    E->native = native;
     E->by_order = true;
     E->dirty = true;
     return VL_OK;

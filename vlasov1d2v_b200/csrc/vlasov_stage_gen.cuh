@@ -27,12 +27,13 @@
 // W and WN are padded so that the k-line loads of the up-to-eight x nodes met by one warp fall
 // in distinct banks (searched at compile time for the actual lane assignment).
 //
-// TMA form (FP64 with 16-byte-aligned state rows, stage_gen_tma_kernel): one thread per CTA loads
-// each array of the tile with one cp.async.bulk.tensor box (no multicast) into the same stages,
-// completing on an mbarrier (bounded waits).  Rows are then contiguous copies of the state: the
-// tile starts at the 16-byte boundary at or below the left v trace, element b's node k sits at
-// column off + 1 + b n + k (off = 0 or 1 per tile), and the column pairs are read as two scalar
-// loads.  Every box lands on a 128-byte-aligned shared-memory address.
+// TMA form (16-byte-aligned state rows, stage_gen_tma_kernel; FP64, and FP32 without the
+// background split): one thread per CTA loads each array of the tile with one
+// cp.async.bulk.tensor box (no multicast) into the same stages, completing on an mbarrier
+// (bounded waits).  Rows are then contiguous copies of the state: the tile starts at the 16-byte
+// boundary at or below the left v trace, element b's node k sits at column off + 1 + b n + k
+// (off < 16 bytes per tile), and the column pairs are read as two scalar loads.  Every box lands
+// on a 128-byte-aligned shared-memory address.
 //
 // Phased form (FP32 rows that are not 16-byte multiples): every thread copies 16-byte chunks
 // with cp.async into contiguous rows, each row starting at the 16-byte boundary at or below the
@@ -172,7 +173,6 @@ struct GenMaps {
 
 template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
 struct GenTmaGeom {
-    static_assert(sizeof(T) == 8, "the TMA form serves FP64 states");
     static constexpr int EPT = EPT_;
     static constexpr int Q = 16 / (int)sizeof(T);                       // elements per 16 bytes
     static constexpr int WB0 = (EPT * N + 2 + 2 * (Q - 1)) / Q * Q;     // tile + both traces, any offset
@@ -200,7 +200,7 @@ struct GenTmaGeom {
         return (s > red ? s : red) + 128;
     }
     static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
-    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * 168);
+    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * (sizeof(T) == 8 ? 168 : 128));
     static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
     static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
     static_assert(WB <= 256, "TMA box width");
@@ -331,7 +331,15 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     }
     const int kind = a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
-    const bool with_bg = GG::BG && a.bg_rb != nullptr;
+    // the TMA form stages no background tables: FP32 contexts with the background split are
+    // launched on another kernel (an error here if one arrives anyway)
+    if constexpr (TMA && GG::BG) {
+        if (a.bg_rb != nullptr) {
+            if (a.err != nullptr && threadIdx.x == 0) atomicOr(a.err, 4);
+            return;
+        }
+    }
+    const bool with_bg = GG::BG && !TMA && a.bg_rb != nullptr;
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile = (g < tiles) ? (tiles - 1 - g) / G + 1 : 0;
@@ -773,10 +781,10 @@ stage_gen_ph_kernel(const StageArgs a, const __grid_constant__ StageTables<float
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
-// TMA form (FP64, 16-byte-aligned state rows)
-template <int N>
-__global__ void __launch_bounds__(GenTmaGeom<N, double>::THREADS, GenTmaGeom<N, double>::MINB)
-stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<double> tb,
+// TMA form (16-byte-aligned state rows; FP32 only without the background split)
+template <int N, typename T>
+__global__ void __launch_bounds__(GenTmaGeom<N, T>::THREADS, GenTmaGeom<N, T>::MINB)
+stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                      const __grid_constant__ GenMaps maps) {
     pdl_wait();
     pdl_trigger();
@@ -784,7 +792,7 @@ stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<doub
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
-    gen_stage_body<N, double, GenGeom<N, double>::EPT, StageTables<double>, true>(
+    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true>(
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
 }
 

@@ -12,7 +12,9 @@ afterwards), and caches the winner per ensemble signature and GPU in a JSON file
 ``(0, native, items_per_cta)`` is the by-order form (``vl_ens_schedule_by_order``): one stage
 launch per order present, each kernel compiled for its order alone, except for the orders whose
 bit n is set in ``native``, whose members run one by one through their own single-problem stage
-kernel (the tensor-core kernel for n = 8); the launches of a stage run on concurrent streams.
+kernel (the tensor-core kernel for n = 8, the generic kernel's TMA form on 16-byte rows);
+``native = VL_ENS_NATIVE_AUTO`` selects the members whose kernels stage tiles by TMA.  The
+launches of a stage run on concurrent streams.
 """
 from __future__ import annotations
 
@@ -27,9 +29,9 @@ import torch
 from . import _device, _lib
 from .timestep import NonFiniteError, get_max_speeds
 
-# by order, order-8 members through the tensor-core single-problem kernel, 8 work items per CTA
-# (the autotuner's choice on B200 for the 64-member benchmark ensemble)
-DEFAULT_SCHEDULE = (0, 1 << 8, 8)
+# by order, the members whose contexts stage tiles by TMA through their own single-problem
+# kernels, 8 work items per CTA
+DEFAULT_SCHEDULE = (0, _lib.VL_ENS_NATIVE_AUTO, 8)
 _CACHE = os.path.join(os.path.expanduser("~"), ".cache", "vlasov1d2v_b200", "ensemble_schedules.json")
 
 
@@ -138,7 +140,7 @@ class Ensemble:
         if candidates is None:
             candidates = [(t, c, k) for t in (128, 64) for c in (1, 2, 3, 4) for k in (1, 2, 4, 8)
                           if not (t == 128 and c > 2)]
-            candidates += [(0, native, k) for native in (0, 1 << 8) for k in (1, 2, 4, 8)]
+            candidates += [(0, native, k) for native in (0, _lib.VL_ENS_NATIVE_AUTO) for k in (1, 2, 4, 8)]
             candidates += [(0, 0x3FE, 8)]   # every order through the single-problem kernels
         snap = self._snapshot()
         trials = []
