@@ -738,7 +738,8 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     }
     // stage kernel (fastest measured per order and precision): the fragment kernel for n = 8; in
     // FP64 the generic kernel for every other order (its TMA form where the rows allow); in FP32
-    // the TMA kernel for n = 4 and the register-pencil kernel otherwise.
+    // the TMA kernel for n = 4, the generic kernel's TMA form on 16-byte rows and the
+    // register-pencil kernel otherwise.
     // VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects one for comparisons
     // FP32 on the generic kernel's phased form (all rows of one j share a 16-byte phase): opt-in
     // with VLASOV1D2V_GEN_PH=1; measured within +-16% of the register-pencil kernel (faster at
