@@ -46,19 +46,24 @@ def test_fp32_background_split_against_fp64(cuda):
     assert ferr_split < ferr_plain / 4
 
 
+@pytest.mark.parametrize("form", ["tma", "phased_bulk"])
 @pytest.mark.parametrize("split", [True, False], ids=["background_split", "plain_fp32"])
-def test_fp32_generic_tma_form_in_the_loop(cuda, split, monkeypatch):
+def test_fp32_generic_tma_form_in_the_loop(cuda, split, form, monkeypatch):
     """FP32 order 6 on 16-byte rows, where the generic kernel's TMA form is the stage kernel:
     without the background split the loop's stages run on it, with the split they go to the
-    register-pencil kernel on its own grid.  Either way 6 steps match a run on the register-pencil
-    kernel alone (VLASOV1D2V_STAGE_KERNEL=pencil)."""
+    register-pencil kernel on its own grid; and the generic kernel's phased rows filled by bulk
+    copies (VLASOV1D2V_GEN_PHB=1, TMA form off), which stage the background tables too.  6 steps
+    match a run on the register-pencil kernel alone (VLASOV1D2V_STAGE_KERNEL=pencil)."""
     from vlasov1d2v_b200 import problem
 
     def run(tma):
-        if tma:
-            monkeypatch.delenv("VLASOV1D2V_STAGE_KERNEL", raising=False)
-        else:
+        for var in ("VLASOV1D2V_STAGE_KERNEL", "VLASOV1D2V_GEN_PHB", "VLASOV1D2V_GEN_NO_TMA"):
+            monkeypatch.delenv(var, raising=False)
+        if not tma:
             monkeypatch.setenv("VLASOV1D2V_STAGE_KERNEL", "pencil")
+        elif form == "phased_bulk":
+            monkeypatch.setenv("VLASOV1D2V_GEN_PHB", "1")
+            monkeypatch.setenv("VLASOV1D2V_GEN_NO_TMA", "1")
         p = problem.build((4, 4, 6), 6, perturbation="cos", amp=0.01, batch_steps=3, precision="fp32",
                           background_split=split)
         p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, 6)

@@ -186,7 +186,7 @@ def test_odd_orders_on_aligned_rows(cuda, n):
         assert rel_err(_np(out)[INNER], want[INNER]) < 1e-14
 
 
-@pytest.mark.parametrize("form", ["pencil", "phased", "tma"])
+@pytest.mark.parametrize("form", ["pencil", "phased", "tma", "phased_bulk"])
 @pytest.mark.parametrize("res", [(2, 2, 3), (2, 2, 4), (2, 2, 2), (2, 3, 6)])
 @pytest.mark.parametrize("n", [3, 5, 6, 7, 9])
 def test_fp32_stage_kernels_other_orders(cuda, n, res, form, monkeypatch):
@@ -194,16 +194,17 @@ def test_fp32_stage_kernels_other_orders(cuda, n, res, form, monkeypatch):
     are 16-byte multiples, (nv + 2) n a multiple of 4; the register-pencil kernel elsewhere), the
     register-pencil kernel everywhere (VLASOV1D2V_STAGE_KERNEL=pencil) and the generic kernel's
     phased form (opt-in VLASOV1D2V_GEN_PH=1 with the TMA form off: rows whose j rows share a
-    16-byte phase, (nu + 2) n (nv + 2) n a multiple of 4).  The three RK stage kinds of a random
-    state against the FP64 oracle, within FP32 rounding of the stage results.  The switches are
-    read when the context is created."""
+    16-byte phase, (nu + 2) n (nv + 2) n a multiple of 4), its rows filled by cp.async or by bulk
+    copies on mbarriers (VLASOV1D2V_GEN_PHB=1).  The three RK stage kinds of a random state
+    against the FP64 oracle, within FP32 rounding of the stage results.  The switches are read
+    when the context is created."""
     from vlasov1d2v_b200 import _lib, problem
     from vlasov1d2v_b200.context import get_context
 
-    for var in ("VLASOV1D2V_GEN_PH", "VLASOV1D2V_GEN_NO_TMA", "VLASOV1D2V_STAGE_KERNEL"):
+    for var in ("VLASOV1D2V_GEN_PH", "VLASOV1D2V_GEN_PHB", "VLASOV1D2V_GEN_NO_TMA", "VLASOV1D2V_STAGE_KERNEL"):
         monkeypatch.delenv(var, raising=False)
-    if form == "phased":
-        monkeypatch.setenv("VLASOV1D2V_GEN_PH", "1")
+    if form in ("phased", "phased_bulk"):
+        monkeypatch.setenv("VLASOV1D2V_GEN_PHB" if form == "phased_bulk" else "VLASOV1D2V_GEN_PH", "1")
         monkeypatch.setenv("VLASOV1D2V_GEN_NO_TMA", "1")
     elif form == "pencil":
         monkeypatch.setenv("VLASOV1D2V_STAGE_KERNEL", "pencil")

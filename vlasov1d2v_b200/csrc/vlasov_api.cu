@@ -281,6 +281,17 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
         }
     }
     if constexpr (sizeof(T) == 4) {
+        if (c->stage_kernel == VL_STAGE_GEN && c->gen_phb) {
+            using G = vl::GenPhGeom<N, float>;
+            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
+                 reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu) |
+                 reinterpret_cast<uintptr_t>(a.u_nodes)) % 16)
+                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
+            return check_launch(launch(c, vl::stage_gen_phb_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s,
+                                       a, tb),
+                                "stage_gen_phb_kernel");
+        }
         if (c->stage_kernel == VL_STAGE_GEN && c->gen_ph) {
             using G = vl::GenPhGeom<N, float>;
             if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
@@ -344,9 +355,18 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool ph) {
+int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool ph, bool phb = false) {
     int blocks = 0;
     if constexpr (sizeof(T) == 4) {
+        if (gen && phb) {   // FP32: the phased rows by bulk copies
+            using G = vl::GenPhGeom<N, float>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_gen_phb_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_phb_kernel<N>, G::THREADS,
+                                                              smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
         if (gen && ph) {   // FP32: the phased form
             using G = vl::GenPhGeom<N, float>;
             const size_t smem = G::smem_bytes();
@@ -418,18 +438,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma, bool ph) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma, bool ph, bool phb = false) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma, ph);
-        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma, ph);
-        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma, ph);
-        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma, ph);
-        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma, ph);
-        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma, ph);
-        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma, ph);
-        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma, ph);
-        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma, ph);
-        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma, ph);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma, ph, phb);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma, ph, phb);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma, ph, phb);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma, ph, phb);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma, ph, phb);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma, ph, phb);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma, ph, phb);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma, ph, phb);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma, ph, phb);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma, ph, phb);
         default: return 1;
     }
 }
@@ -758,11 +778,17 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     }();
     const bool gen_tma32 = cfg->precision == VL_FP32 && ((size_t)(cfg->nv + 2) * n) % 4 == 0 && !no_gen_tma &&
                            encode_fn() != nullptr;
-    c->stage_kernel = c->use_frag                    ? VL_STAGE_FRAG
-                      : cfg->precision == VL_FP64    ? VL_STAGE_GEN
-                      : c->use_tma                   ? VL_STAGE_TMA
-                      : (c->gen_ph || gen_tma32)     ? VL_STAGE_GEN
-                                                     : VL_STAGE_PENCIL;
+    // FP32 rows that are not 16-byte multiples but share a phase per j (as the phased form):
+    // the phased rows filled by bulk copies on mbarriers, opt-in with VLASOV1D2V_GEN_PHB=1
+    {
+        const char *env = getenv("VLASOV1D2V_GEN_PHB");
+        c->gen_phb = cfg->precision == VL_FP32 && ph_ok && !gen_tma32 && env && env[0] == '1';
+    }
+    c->stage_kernel = c->use_frag                                  ? VL_STAGE_FRAG
+                      : cfg->precision == VL_FP64                  ? VL_STAGE_GEN
+                      : c->use_tma                                 ? VL_STAGE_TMA
+                      : (c->gen_ph || gen_tma32 || c->gen_phb)     ? VL_STAGE_GEN
+                                                                   : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
         if (env) {
@@ -779,10 +805,12 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even), FP32 as above
     c->gen_tma = gen && (cfg->precision == VL_FP64 ? ((size_t)(cfg->nv + 2) * n) % 2 == 0 : gen_tma32) &&
                  encode_fn() != nullptr && !no_gen_tma;
-    c->gen_ph = c->gen_ph && gen && !c->gen_tma;
+    c->gen_phb = c->gen_phb && gen && !c->gen_tma;
+    c->gen_ph = c->gen_ph && gen && !c->gen_tma && !c->gen_phb;
     const int occ = cfg->precision == VL_FP64
                         ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma, false)
-                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma, c->gen_ph);
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma, c->gen_ph,
+                                                 c->gen_phb);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double

@@ -41,6 +41,7 @@ struct vl_ctx {
     int stage_kernel = VL_STAGE_GEN;   // which stage kernel the launches use (vl_stage_kernel)
     bool gen_tma = false;         // generic stage kernel in its TMA form (FP64, aligned rows)
     bool gen_ph = false;          // generic stage kernel in its phased form (FP32)
+    bool gen_phb = false;         // the phased rows filled by bulk copies on mbarriers (FP32)
     bool use_pdl = false;         // loop launches with programmatic dependent launch
     bool pdl_now = false;         // set while vl_ssp_rk3_steps issues its launches
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)

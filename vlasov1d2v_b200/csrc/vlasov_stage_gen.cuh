@@ -277,11 +277,13 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PH = false>
+template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PH = false, bool BULK = false>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
                                                int g, int G, unsigned char *smem,
                                                const GenMaps *maps = nullptr) {
+    static_assert(!BULK || PH, "bulk copies fill the phased rows");
     constexpr bool CONTIG = TMA || PH;   // contiguous rows (scalar pair loads)
+    constexpr bool MB = TMA || BULK;     // stages filled by asynchronous bulk copies on mbarriers
     using GG = GenGeom<N, T, EPT>;
     using V2 = typename GenPair<T>::V;
     constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
@@ -353,7 +355,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     }
     __syncthreads();
 
-    if constexpr (TMA) {
+    if constexpr (MB) {
         if (tid == 0) {
             mbar_init(&gfull[0], 1);
             mbar_init(&gfull[1], 1);
@@ -485,6 +487,91 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             (void)tt;
         }
     };
+    // phased rows by bulk copies (warp 0): the same row runs as the phased form, each one
+    // cp.async.bulk from its 16-byte boundary (16-byte multiples), completing on gfull[s] with
+    // the exact byte total announced first; the u nodes from the even index at or below Ag n
+    auto issue_phb = [&](int s, int tt) {
+        if constexpr (BULK) {
+            using GP = GenPhGeom<N, T, EPT>;
+            const int au = tt / nbt;
+            const int b0 = (tt - au * nbt) * EPT;
+            const int nb = min(EPT, nv - b0);
+            const int Ag = au + 1;
+            const size_t cg0 = (size_t)(b0 + 1) * N - 1;
+            const int wc = nb * N + 2;   // the tile's elements and both v traces (<= GP::WC)
+            unsigned char *st = stage_ptr(s);
+            T *dIn = reinterpret_cast<T *>(st);
+            T *dFn = reinterpret_cast<T *>(st + S_IN);
+            T *dXF = reinterpret_cast<T *>(st + S_IN + S_FN);
+            T *dUF = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF);
+            T *dBG = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF + S_UF);
+            double *dUX = reinterpret_cast<double *>(st + S_IN + S_FN + S_XF + S_UF + S_BG);
+            auto sr = [&](int ee, int ii, int aa, int jj) -> size_t {
+                return (((size_t)ee * N + ii) * U + aa) * N + jj;
+            };
+            const int n_in = N * N, n_fn = with_fn ? N * N : 0, n_bg = with_bg ? 2 * N : 0;
+            const int nrow = n_in + n_fn + 4 * N + n_bg;
+            // row q of the tile: its shared destination, source array and row index
+            auto row_of = [&](int q, T *&dst, const T *&src, size_t &r) {
+                if (q < n_in + n_fn) {
+                    const int qq = q < n_in ? q : q - n_in;
+                    const int ii = qq / N, jj = qq - (qq / N) * N;
+                    dst = (q < n_in ? dIn : dFn) + ii * GP::PS + jj * GP::RS;
+                    src = q < n_in ? in : fn;
+                    r = sr(Eg, ii, Ag, jj);
+                    return;
+                }
+                q -= n_in + n_fn;
+                if (q < 4 * N) {
+                    const int side = (q / N) & 1, qq = q % N;
+                    src = in;
+                    if (q < 2 * N) {   // x traces: row j = qq of (El, i = n-1) / (Er, i = 0)
+                        dst = dXF + (side * N + qq) * GP::RS;
+                        r = sr(side ? Er : El, side ? 0 : N - 1, Ag, qq);
+                    } else {           // u traces: row i = qq of (a-1, j = n-1) / (a+1, j = 0)
+                        dst = dUF + (side * N + qq) * GP::RS;
+                        r = sr(Eg, qq, side ? Ag + 1 : Ag - 1, side ? 0 : N - 1);
+                    }
+                    return;
+                }
+                q -= 4 * N;
+                const int tbl = q / N, jj = q % N;   // background-split tables [U n][V n]
+                dst = dBG + (tbl * N + jj) * GP::RS;
+                src = reinterpret_cast<const T *>(tbl ? a.bg_rb : a.bg_eu);
+                r = (size_t)Ag * N + jj;
+            };
+            auto span = [&](size_t r, size_t &s0) -> uint32_t {
+                const size_t a0 = r * (size_t)sJ + cg0;
+                s0 = a0 & ~(size_t)3;
+                return (uint32_t)(((a0 - s0 + wc + 3) >> 2) * 16);
+            };
+            const uint32_t ux_bytes = (uint32_t)sizeof(double) * (N + (N & 1));
+            uint32_t total = 0;
+            for (int q = lane; q < nrow; q += 32) {
+                T *dst;
+                const T *src;
+                size_t r, s0;
+                row_of(q, dst, src, r);
+                total += span(r, s0);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
+            if (lane == 0) mbar_arrive_expect_tx(&gfull[s], total + ux_bytes);
+            __syncwarp();
+            for (int q = lane; q < nrow; q += 32) {
+                T *dst;
+                const T *src;
+                size_t r, s0;
+                row_of(q, dst, src, r);
+                const uint32_t bytes = span(r, s0);
+                bulk_load(dst, src + s0, bytes, &gfull[s]);
+            }
+            if (lane == 0) bulk_load(dUX, a.u_nodes + ((Ag * N) & ~1), ux_bytes, &gfull[s]);
+        } else {
+            (void)s;
+            (void)tt;
+        }
+    };
     // TMA form: one thread loads the tile's boxes into stage s
     auto issue_tma = [&](int s, int tt) {
         if constexpr (TMA) {
@@ -534,6 +621,11 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             if (ntile > 0) issue_tma(0, g);
             if (ntile > 1) issue_tma(1, g + G);
         }
+    } else if constexpr (BULK) {
+        if (warp == 0) {
+            if (ntile > 0) issue_phb(0, g);
+            if (ntile > 1) issue_phb(1, g + G);
+        }
     } else {
 #pragma unroll
         for (int s0 = 0; s0 < NST - 1; ++s0) {
@@ -547,7 +639,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         }
     }
     for (int q = 0; q < ntile; ++q) {
-        if constexpr (!TMA) {
+        if constexpr (!MB) {
             const int qn = q + NST - 1;
             if (qn < ntile) {
                 if constexpr (PH)
@@ -565,7 +657,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         const bool act = has_item && b < nb;
         const int col = (b0 + b + 1) * N + 2 * p;    // global v-node column of the pair
         const double vn0 = act ? a.v_nodes[col] : 0.0, vn1 = act ? a.v_nodes[col + 1] : 0.0;
-        if constexpr (TMA) {
+        if constexpr (MB) {
             if (!mbar_wait_bounded(&gfull[q & 1], (uint32_t)((q >> 1) & 1))) {
                 if (a.err != nullptr) atomicOr(a.err, 2);
                 return;
@@ -599,7 +691,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         };
         const int ush0 = PH ? ((K0 - KJ) & 3) : 0;
         const int ush1 = PH ? ((K0 + N * KJ) & 3) : 0;
-        const double *sUX = sUX0 + (TMA ? ((Ag * N) & 1) : 0);
+        const double *sUX = sUX0 + (MB ? ((Ag * N) & 1) : 0);
         auto ld2 = [&](const T *q2) -> V2 {
             if constexpr (CONTIG) {
                 V2 r;
@@ -736,6 +828,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         __syncthreads();   // stage q % NST consumed before it is refilled
         if constexpr (TMA) {
             if (tid == 0 && q + 2 < ntile) issue_tma(q & 1, g + (q + 2) * G);
+        } else if constexpr (BULK) {
+            if (warp == 0 && q + 2 < ntile) issue_phb(q & 1, g + (q + 2) * G);
         }
     }
     cp_async_wait<0>();
@@ -778,6 +872,20 @@ stage_gen_ph_kernel(const StageArgs a, const __grid_constant__ StageTables<float
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
     gen_stage_body<N, float, GenGeom<N, float>::EPT, StageTables<float>, false, true>(
+        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
+}
+
+// phased rows filled by bulk copies on mbarriers (FP32, any row alignment)
+template <int N>
+__global__ void __launch_bounds__(GenPhGeom<N, float>::THREADS, GenPhGeom<N, float>::MINB)
+stage_gen_phb_kernel(const StageArgs a, const __grid_constant__ StageTables<float> tb) {
+    pdl_wait();
+    pdl_trigger();
+    if (a.state != nullptr && a.state->active == 0) return;
+    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
+    gen_stage_body<N, float, GenGeom<N, float>::EPT, StageTables<float>, false, true, true>(
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
