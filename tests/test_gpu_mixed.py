@@ -49,11 +49,10 @@ def test_fp32_background_split_against_fp64(cuda):
 @pytest.mark.parametrize("form", ["tma", "phased_bulk"])
 @pytest.mark.parametrize("split", [True, False], ids=["background_split", "plain_fp32"])
 def test_fp32_generic_tma_form_in_the_loop(cuda, split, form, monkeypatch):
-    """FP32 order 6 on 16-byte rows, where the generic kernel's TMA form is the stage kernel:
-    without the background split the loop's stages run on it, with the split they go to the
-    register-pencil kernel on its own grid; and the generic kernel's phased rows filled by bulk
-    copies (VLASOV1D2V_GEN_PHB=1, TMA form off), which stage the background tables too.  6 steps
-    match a run on the register-pencil kernel alone (VLASOV1D2V_STAGE_KERNEL=pencil)."""
+    """FP32 order 6 on 16-byte rows, where the generic kernel's TMA form is the stage kernel (with
+    the background split it stages the two background tables as 2-D boxes), and the generic
+    kernel's phased rows filled by bulk copies (VLASOV1D2V_GEN_PHB=1, TMA form off).  6 steps with
+    and without the split match a run on the register-pencil kernel (VLASOV1D2V_STAGE_KERNEL=pencil)."""
     from vlasov1d2v_b200 import problem
 
     def run(tma):

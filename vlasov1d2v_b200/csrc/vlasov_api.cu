@@ -210,6 +210,35 @@ int gen_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
     return VL_OK;
 }
 
+// 2-D view [U n][V n] of a background-split table for the generic kernel's TMA form (FP32),
+// box (WB, n): the tile's rows of one u element
+template <int N, typename T>
+int gen_bg_map(vl_ctx *c, const float *ptr, CUtensorMap *out) {
+    using G = vl::GenTmaGeom<N, T>;
+    auto key = std::make_pair(static_cast<const void *>(ptr), 30);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2;
+    cuuint64_t dims[2] = {V * N, U * N};
+    cuuint64_t strides[1] = {V * N * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)G::WB, (cuuint32_t)N};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (generic kernel, background) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
 template <int N, typename T>
 int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageTables<T> tb;
@@ -231,11 +260,7 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
         }
     vl::StageArgs a = a0;
     if (a.err == nullptr) a.err = c->d_err;
-    // FP32 with the background split has no TMA form of the generic kernel: the register-pencil
-    // kernel takes those launches, on its own grid
-    const bool gen_tma_now = c->stage_kernel == VL_STAGE_GEN && c->gen_tma && (sizeof(T) == 8 || a.bg_rb == nullptr);
-    const bool bg_fallback = c->stage_kernel == VL_STAGE_GEN && c->gen_tma && !gen_tma_now;
-    dim3 grid(bg_fallback ? c->stage_grid_g_bg : c->stage_grid_g, c->cfg.nx);
+    dim3 grid(c->stage_grid_g, c->cfg.nx);
     if constexpr (N == 8) {
         if (c->use_frag) {
             using G = vl::FragGeom<T>;
@@ -257,28 +282,26 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                                 "stage_frag_kernel");
         }
     }
-    if (bg_fallback) {
-        using G = vl::PencilGeom<N, T>;
-        return check_launch(launch(c, vl::stage_pencil_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
-                                   tb),
-                            "stage_pencil_kernel");
-    }
-    {
-        if (gen_tma_now) {
-            using G = vl::GenTmaGeom<N, T>;
-            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
-                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out)) % 16)
-                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
-            vl::GenMaps maps;
-            int rc;
-            if ((rc = gen_map<N, T>(c, a.in, 0, &maps.in_tile))) return rc;
-            if ((rc = gen_map<N, T>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
-            if ((rc = gen_map<N, T>(c, a.in, 1, &maps.xface))) return rc;
-            if ((rc = gen_map<N, T>(c, a.in, 2, &maps.uface))) return rc;
-            return check_launch(launch(c, vl::stage_gen_tma_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(),
-                                       s, a, tb, maps),
-                                "stage_gen_tma_kernel");
+    if (c->stage_kernel == VL_STAGE_GEN && c->gen_tma) {
+        using G = vl::GenTmaGeom<N, T>;
+        if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+             reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
+             reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu)) % 16)
+            return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
+        vl::GenMaps maps;
+        std::memset(&maps, 0, sizeof(maps));
+        int rc;
+        if ((rc = gen_map<N, T>(c, a.in, 0, &maps.in_tile))) return rc;
+        if ((rc = gen_map<N, T>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
+        if ((rc = gen_map<N, T>(c, a.in, 1, &maps.xface))) return rc;
+        if ((rc = gen_map<N, T>(c, a.in, 2, &maps.uface))) return rc;
+        if (sizeof(T) == 4 && a.bg_rb != nullptr) {
+            if ((rc = gen_bg_map<N, T>(c, a.bg_eu, &maps.bg_eu))) return rc;
+            if ((rc = gen_bg_map<N, T>(c, a.bg_rb, &maps.bg_rb))) return rc;
         }
+        return check_launch(launch(c, vl::stage_gen_tma_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
+                                   tb, maps),
+                            "stage_gen_tma_kernel");
     }
     if constexpr (sizeof(T) == 4) {
         if (c->stage_kernel == VL_STAGE_GEN && c->gen_phb) {
@@ -572,8 +595,7 @@ int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
 
 // byte offset of the field scratch inside a loop workspace (after the moment partials)
 size_t partials_bytes(const vl_ctx *c) {
-    int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
-    if (c->stage_grid_g_bg > g) g = c->stage_grid_g_bg;
+    const int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
     const size_t b = sizeof(double) * (size_t)c->cfg.nx * g * c->cfg.n;
     return (b + 255) & ~(size_t)255;
 }
@@ -770,8 +792,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         c->gen_ph = cfg->precision == VL_FP32 && ph_ok && env && env[0] == '1';
     }
     // FP32 on the generic kernel's TMA form where the rows are 16-byte multiples ((nv+2) n a
-    // multiple of 4), orders other than 4 and 8 (launches with the background split go to the
-    // register-pencil kernel); VLASOV1D2V_GEN_NO_TMA=1 switches the TMA form off
+    // multiple of 4), orders other than 4 and 8; VLASOV1D2V_GEN_NO_TMA=1 switches it off
     const bool no_gen_tma = [] {
         const char *env = getenv("VLASOV1D2V_GEN_NO_TMA");
         return env && env[0] == '1';
@@ -819,16 +840,6 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if (g > tiles) g = tiles;
     if (g < 1) g = 1;
     c->stage_grid_g = g;
-    c->stage_grid_g_bg = g;
-    if (cfg->precision == VL_FP32 && c->gen_tma) {   // the register-pencil kernel's own grid
-        const int occ_p = stage_occupancy<float>(n, false, false, false, false, false);
-        const int bp = 32 / n > 0 ? 32 / n : 1;
-        const int tiles_p = cfg->nu * ((cfg->nv + bp - 1) / bp);
-        int gp = (c->sm_count * occ_p) / cfg->nx;
-        if (gp > tiles_p) gp = tiles_p;
-        if (gp < 1) gp = 1;
-        c->stage_grid_g_bg = gp;
-    }
     // standalone moment: MOMENT_CTAS_PER_SM resident CTAs per SM, at most one per u element
     int gm = (c->sm_count * vl::MOMENT_CTAS_PER_SM) / cfg->nx;
     if (gm > cfg->nu) gm = cfg->nu;
@@ -1013,9 +1024,7 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     cudaStream_t s = as_stream(stream);
     double *partials = static_cast<double *>(workspace);
     double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) + partials_bytes(c));
-    // FP32 with the background split on a generic-TMA context: the register-pencil kernel's grid
-    const int G = (c->cfg.precision == VL_FP32 && c->gen_tma && c->bg_rb != nullptr) ? c->stage_grid_g_bg
-                                                                                       : c->stage_grid_g;
+    const int G = c->stage_grid_g;
     int rc;
     // the field solve's ticket counter starts at zero (the last CTA of each record resets it)
     VL_CUDA(cudaMemsetAsync(fscratch + 4 * (size_t)c->cfg.n_modes, 0, sizeof(int), s));

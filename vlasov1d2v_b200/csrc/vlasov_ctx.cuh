@@ -18,8 +18,6 @@ struct vl_ctx {
     int device;
     int sm_count;
     int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
-    int stage_grid_g_bg;   // the same for FP32 launches with the background split when the
-                           // generic kernel's TMA form (no background tables) is the stage kernel
     int moment_grid_g;  // CTAs per x element of the standalone moment kernel
     double up[vl::NMAX * vl::NMAX];
     double xi[vl::NMAX * 2];

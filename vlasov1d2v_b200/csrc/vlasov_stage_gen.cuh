@@ -27,9 +27,9 @@
 // W and WN are padded so that the k-line loads of the up-to-eight x nodes met by one warp fall
 // in distinct banks (searched at compile time for the actual lane assignment).
 //
-// TMA form (16-byte-aligned state rows, stage_gen_tma_kernel; FP64, and FP32 without the
-// background split): one thread per CTA loads each array of the tile with one
-// cp.async.bulk.tensor box (no multicast) into the same stages, completing on an mbarrier
+// TMA form (16-byte-aligned state rows, stage_gen_tma_kernel; FP64 and FP32, the FP32
+// background-split tables as two 2-D boxes): one thread per CTA loads each array of the tile with
+// one cp.async.bulk.tensor box (no multicast) into the same stages, completing on an mbarrier
 // (bounded waits).  Rows are then contiguous copies of the state: the tile starts at the 16-byte
 // boundary at or below the left v trace, element b's node k sits at column off + 1 + b n + k
 // (off < 16 bytes per tile), and the column pairs are read as two scalar loads.  Every box lands
@@ -169,6 +169,8 @@ struct GenMaps {
     CUtensorMap fn_tile;   // the same box over f^n
     CUtensorMap xface;     // box (WB, n, 1, 1, 1): one x node plane
     CUtensorMap uface;     // box (WB, 1, 1, n, 1): one j row of every x node
+    CUtensorMap bg_eu;     // FP32 background-split tables [U n][V n]: box (WB, n)
+    CUtensorMap bg_rb;
 };
 
 template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
@@ -189,10 +191,14 @@ struct GenTmaGeom {
     static constexpr size_t FSIDE_B = al(sizeof(T) * (size_t)N * WB);
     static constexpr size_t XF_B = 2 * FSIDE_B;
     static constexpr size_t UF_B = XF_B;
+    // FP32: the two background-split tables' rows of the tile, each table on a 128-byte boundary
+    static constexpr size_t BGSIDE_B = sizeof(T) == 4 ? al(sizeof(float) * (size_t)N * WB) : 0;
+    static constexpr size_t BG_B = 2 * BGSIDE_B;
     static constexpr size_t UX_B = al(sizeof(double) * (size_t)UXC);
-    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + UX_B;
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
     static constexpr uint32_t TX_IN = sizeof(T) * WB * RJ * N;
     static constexpr uint32_t TX_FACE = sizeof(T) * WB * N;
+    static constexpr uint32_t TX_BG = sizeof(float) * WB * N;
     static constexpr uint32_t TX_UX = sizeof(double) * UXC;
     static constexpr size_t smem_bytes() {
         const size_t s = NST * STAGE_B;
@@ -242,6 +248,7 @@ struct GenLayout {
     using GG = GenGeom<N, T, EPT>;
     static constexpr int RIN = GG::W, PIN = GG::PS, RFN = GG::WN, PFN = GG::PSF, RFC = GG::WF, Q = 1;
     static constexpr int FS = N * GG::WF;   // offset of the second face side (elements)
+    static constexpr int BGS = N * GG::WF;  // offset of the second background table (floats)
     static constexpr size_t S_IN = GG::IN_B, S_FN = GG::FN_B, S_XF = GG::XF_B, S_UF = GG::UF_B;
     static constexpr size_t S_BG = GG::BG_B, S_STAGE = GG::STAGE_B;
 };
@@ -250,6 +257,7 @@ struct GenLayout<2, N, T, EPT> {
     using GP = GenPhGeom<N, T, EPT>;
     static constexpr int RIN = GP::RS, PIN = GP::PS, RFN = GP::RS, PFN = GP::PS, RFC = GP::RS, Q = 4;
     static constexpr int FS = N * GP::RS;
+    static constexpr int BGS = N * GP::RS;
     static constexpr size_t S_IN = GP::IN_B, S_FN = GP::FN_B, S_XF = GP::XF_B, S_UF = GP::UF_B;
     static constexpr size_t S_BG = GP::BG_B, S_STAGE = GP::STAGE_B;
 };
@@ -258,8 +266,9 @@ struct GenLayout<1, N, T, EPT> {
     using GT = GenTmaGeom<N, T, EPT>;
     static constexpr int RIN = GT::WB, PIN = GT::PS, RFN = GT::WB, PFN = GT::PS, RFC = GT::WB, Q = GT::Q;
     static constexpr int FS = (int)(GT::FSIDE_B / sizeof(T));
+    static constexpr int BGS = (int)(GT::BGSIDE_B / sizeof(float));
     static constexpr size_t S_IN = GT::IN_B, S_FN = GT::FN_B, S_XF = GT::XF_B, S_UF = GT::UF_B;
-    static constexpr size_t S_BG = 0, S_STAGE = GT::STAGE_B;
+    static constexpr size_t S_BG = GT::BG_B, S_STAGE = GT::STAGE_B;
 };
 
 template <typename T>
@@ -333,15 +342,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     }
     const int kind = a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
-    // the TMA form stages no background tables: FP32 contexts with the background split are
-    // launched on another kernel (an error here if one arrives anyway)
-    if constexpr (TMA && GG::BG) {
-        if (a.bg_rb != nullptr) {
-            if (a.err != nullptr && threadIdx.x == 0) atomicOr(a.err, 4);
-            return;
-        }
-    }
-    const bool with_bg = GG::BG && !TMA && a.bg_rb != nullptr;
+    const bool with_bg = GG::BG && a.bg_rb != nullptr;
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile = (g < tiles) ? (tiles - 1 - g) / G + 1 : 0;
@@ -583,7 +584,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             unsigned char *st = stage_ptr(s);
             unsigned char *xf = st + S_IN + S_FN;
             unsigned char *uf = xf + S_XF;
-            const uint32_t tx = GT::TX_IN * (with_fn ? 2 : 1) + 4 * GT::TX_FACE + GT::TX_UX;
+            const uint32_t tx = GT::TX_IN * (with_fn ? 2 : 1) + 4 * GT::TX_FACE + GT::TX_UX +
+                                (with_bg ? 2 * GT::TX_BG : 0);
             mbar_arrive_expect_tx(&gfull[s], tx);
             tma_load_5d(st, &maps->in_tile, &gfull[s], xs, 0, Ag, 0, Eg);
             if (with_fn) tma_load_5d(st + S_IN, &maps->fn_tile, &gfull[s], xs, 0, Ag, 0, Eg);
@@ -591,7 +593,11 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             tma_load_5d(xf + GT::FSIDE_B, &maps->xface, &gfull[s], xs, 0, Ag, 0, Er);
             tma_load_5d(uf, &maps->uface, &gfull[s], xs, N - 1, Ag - 1, 0, Eg);
             tma_load_5d(uf + GT::FSIDE_B, &maps->uface, &gfull[s], xs, 0, Ag + 1, 0, Eg);
-            bulk_load(uf + S_UF, a.u_nodes + ((Ag * N) & ~1), GT::TX_UX, &gfull[s]);
+            if (with_bg) {
+                tma_load_2d(uf + S_UF, &maps->bg_eu, &gfull[s], xs, Ag * N);
+                tma_load_2d(uf + S_UF + GT::BGSIDE_B, &maps->bg_rb, &gfull[s], xs, Ag * N);
+            }
+            bulk_load(uf + S_UF + S_BG, a.u_nodes + ((Ag * N) & ~1), GT::TX_UX, &gfull[s]);
         } else {
             (void)s;
             (void)tt;
@@ -781,10 +787,10 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     const float *pbg = sBG + j * RFC + cfc + jsh(j);
                     if constexpr (CONTIG) {
                         eu = make_float2(pbg[0], pbg[1]);
-                        rb = make_float2(pbg[N * RFC], pbg[N * RFC + 1]);
+                        rb = make_float2(pbg[L::BGS], pbg[L::BGS + 1]);
                     } else {
                         eu = *reinterpret_cast<const float2 *>(pbg);
-                        rb = *reinterpret_cast<const float2 *>(pbg + N * RFC);
+                        rb = *reinterpret_cast<const float2 *>(pbg + L::BGS);
                     }
                     r0 += (T)fmaf((float)Ei, eu.x, rb.x);
                     r1 += (T)fmaf((float)Ei, eu.y, rb.y);
@@ -889,7 +895,7 @@ stage_gen_phb_kernel(const StageArgs a, const __grid_constant__ StageTables<floa
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
-// TMA form (16-byte-aligned state rows; FP32 only without the background split)
+// TMA form (16-byte-aligned state rows)
 template <int N, typename T>
 __global__ void __launch_bounds__(GenTmaGeom<N, T>::THREADS, GenTmaGeom<N, T>::MINB)
 stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
