@@ -30,8 +30,8 @@ from . import _device, _lib
 from .timestep import NonFiniteError, get_max_speeds
 
 # by order, the members whose contexts stage tiles by TMA through their own single-problem
-# kernels, 8 work items per CTA
-DEFAULT_SCHEDULE = (0, _lib.VL_ENS_NATIVE_AUTO, 8)
+# kernels, 2 work items per CTA (the autotuner's choice on B200 for the 64-member benchmark)
+DEFAULT_SCHEDULE = (0, _lib.VL_ENS_NATIVE_AUTO, 2)
 _CACHE = os.path.join(os.path.expanduser("~"), ".cache", "vlasov1d2v_b200", "ensemble_schedules.json")
 
 
