@@ -173,6 +173,11 @@ struct GenMaps {
     CUtensorMap bg_rb;
 };
 
+// register budget per thread of the FP32 TMA form (resident CTAs requested from the compiler)
+#ifndef VL_GEN_TMA_REG32
+#define VL_GEN_TMA_REG32 128
+#endif
+
 template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
 struct GenTmaGeom {
     static constexpr int EPT = EPT_;
@@ -206,7 +211,7 @@ struct GenTmaGeom {
         return (s > red ? s : red) + 128;
     }
     static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
-    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * (sizeof(T) == 8 ? 168 : 128));
+    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * (sizeof(T) == 8 ? 168 : VL_GEN_TMA_REG32));
     static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
     static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
     static_assert(WB <= 256, "TMA box width");
