@@ -1,0 +1,67 @@
+// Host-side check of the shared-memory and tensor-copy geometry of the generic stage kernel's
+// TMA and phased forms, for every compiled order and both precisions: box widths within the
+// tensor-copy limit and 16-byte multiples, every staged array on a 128-byte boundary, the stage
+// ring within the shared memory of one CTA.  Prints one line per failure and "ALL OK" otherwise.
+#include <cstdio>
+
+#include "vlasov_stage_gen.cuh"
+
+static int failures = 0;
+
+static void expect(bool ok, const char *what, int n, int es) {
+    if (!ok) {
+        std::printf("FAIL n=%d element=%dB: %s\n", n, es, what);
+        ++failures;
+    }
+}
+
+template <int N, typename T>
+void check_tma() {
+    using G = vl::GenTmaGeom<N, T>;
+    const int es = (int)sizeof(T);
+    expect(G::WB % G::Q == 0, "TMA row width is a whole number of 16-byte units", N, es);
+    expect(G::WB <= 256, "TMA box width <= 256 elements", N, es);
+    expect((G::WB * sizeof(T)) % 16 == 0, "TMA box inner extent is a 16-byte multiple", N, es);
+    expect(G::RJ >= N, "rows per plane cover the j extent", N, es);
+    expect(G::WB >= G::EPT * N + 2 + (G::Q - 1), "row holds the tile, both traces and the alignment offset", N, es);
+    expect(G::IN_B % 128 == 0 && G::FN_B % 128 == 0 && G::FSIDE_B % 128 == 0 && G::XF_B % 128 == 0 &&
+               G::UF_B % 128 == 0 && G::BGSIDE_B % 128 == 0 && G::UX_B % 128 == 0 && G::STAGE_B % 128 == 0,
+           "every staged array starts on a 128-byte boundary", N, es);
+    expect(G::UX_B >= sizeof(double) * (size_t)G::UXC, "u-node slot holds the even-aligned copy", N, es);
+    expect(G::smem_bytes() <= 227 * 1024, "stage ring fits the shared memory of one CTA", N, es);
+}
+
+template <int N>
+void check_ph() {
+    using G = vl::GenPhGeom<N, float>;
+    expect(G::RS % 4 == 0, "phased row slot is a whole number of 16-byte units", N, 4);
+    // the longest copied run: from the 16-byte boundary up to 3 floats below the left trace through
+    // the right trace, in whole 16-byte units
+    expect(G::RS >= (G::WC + 6) / 4 * 4, "phased row slot holds the run from any 16-byte phase", N, 4);
+    expect(G::IN_B % 128 == 0 && G::XF_B % 128 == 0 && G::BG_B % 128 == 0 && G::UX_B % 128 == 0,
+           "every phased array starts on a 128-byte boundary", N, 4);
+    expect(G::UX_B >= sizeof(double) * (size_t)(N + (N & 1)), "u-node slot holds the even-aligned copy", N, 4);
+    expect(G::smem_bytes() <= 227 * 1024, "phased stage ring fits the shared memory of one CTA", N, 4);
+}
+
+template <int N>
+void check_order() {
+    check_tma<N, double>();
+    check_tma<N, float>();
+    check_ph<N>();
+}
+
+int main() {
+    check_order<1>();
+    check_order<2>();
+    check_order<3>();
+    check_order<4>();
+    check_order<5>();
+    check_order<6>();
+    check_order<7>();
+    check_order<8>();
+    check_order<9>();
+    check_order<10>();
+    if (failures == 0) std::printf("ALL OK\n");
+    return failures == 0 ? 0 : 1;
+}
