@@ -2,7 +2,7 @@
 
 The field energy of a linearly unstable run grows as W(t) ~ exp(2 gamma t) once the fastest
 mode dominates, so gamma is half the least-squares slope of ln W over that window.  These
-helpers judge the mixed-precision form against the FP64 plain form on the same problem.
+helpers compare the mixed-precision form against the FP64 plain form on the same problem.
 """
 import numpy as np
 

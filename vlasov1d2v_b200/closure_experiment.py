@@ -1,4 +1,4 @@
-"""The learned-closure experiment: train on fine runs, judge on a held-out fine run.
+"""The learned-closure experiment: train on fine runs, evaluate on a held-out fine run.
 
     python -m vlasov1d2v_b200.closure_experiment [--draws 4] [--snapshots 8] [--every 25]
 
@@ -149,7 +149,7 @@ def main(argv=None):
         win = (0.5 * args.t_end, args.t_end)
     g_f = growth_rate(tf, wf, *win)[0]
 
-    def judge(t, w, f):
+    def score(t, w, f):
         g = growth_rate(np.asarray(t), np.asarray(w), *win)[0]
         fi = f[1:-1, :, 1:-1, :, 1:-1, :].double()
         # compare at (about) the same final time: the coarse runs stop at their own last step
@@ -159,14 +159,14 @@ def main(argv=None):
 
     out.update({"growth_window": list(win), "growth_rate_fine": g_f, "fine_final_time": float(tf[-1]),
                 "fine_steps": int(fine.stepper.steps_counter), "coarse_steps": int(nsteps),
-                "plain": judge(plain.stepper.time_array, plain.stepper.field_energy, plain.f.arr)})
+                "plain": score(plain.stepper.time_array, plain.stepper.field_energy, plain.f.arr)})
     runs = []
     for alpha in args.alpha:
         _, cl = _problems(q, fine_res, coarse_res)
         cs = ClosureStepper(cl, mlp=mlp, escale=escale, alpha=alpha)
         sec = _timed(lambda: cs.run_steps(nsteps, batch=50))
         rec = {"alpha": alpha, "closure_s": sec, "fallback_step": cs.fallback_step,
-               "speedup_vs_fine": out["fine_s"] / sec, **judge(cs.times, cs.energies, cl.f.arr)}
+               "speedup_vs_fine": out["fine_s"] / sec, **score(cs.times, cs.energies, cl.f.arr)}
         _log(rec)
         runs.append(rec)
         del cs, cl
