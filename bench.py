@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 METRIC = "phase-space DOF-updates/s per RK3 step, FP64 plain vs FP32 mixed; HBM roofline %"
 RES = (32, 50, 50)
 ORDER = 8
-SAMPLE_RES = (4, 50, 50)  # CPU sample: the same velocity grid, 4 of the 32 x elements
+SAMPLE_RES = (4, 50, 50)  # labelled extra CPU sample: the same velocity grid, 4 of the 32 x elements
 
 
 def parse():
@@ -103,12 +103,14 @@ def dof(res, n):
 # ----------------------------------------------------------------------------------------------
 # CPU (oracle port) timing: the reference arm and the cpu_baseline object
 # ----------------------------------------------------------------------------------------------
-def cpu_port_rate(steps, warmup):
+def cpu_port_rate(steps, warmup, res=RES):
+    """Steps of the oracle port (NumPy FP64 restatement of the reference step, BLAS on every host
+    core) on the benchmark grid itself: DOF-updates/s, seconds per step, cores."""
     import numpy as np
 
     from oracle import vlasov_oracle as vo
 
-    c = vo.make_case(*SAMPLE_RES, ORDER)
+    c = vo.make_case(*res, ORDER)
     f = vo.cos_perturbed(c, c.extra["norm"].vt_e, 6, 1.0e-3, noise=1.0e-6, seed=0)
     rho = vo.moment_zero(f, c)
     E0, _ = vo.poisson2(rho - np.mean(rho), c)
@@ -120,7 +122,7 @@ def cpu_port_rate(steps, warmup):
         _, dt = vo.ssp_rk3_step(f, dt, c)
     t = (time.perf_counter() - t0) / max(steps, 1)
     cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    return dof(SAMPLE_RES, ORDER) / t, t, cores
+    return dof(res, ORDER) / t, t, cores
 
 
 def measure_ensemble(steps, warmup, members=64, seed=0, schedule=None):
@@ -175,13 +177,17 @@ def measure_ensemble(steps, warmup, members=64, seed=0, schedule=None):
                         "<= 2.4M DOF each"}
 
 
-def cpu_baseline_obj(steps=3, warmup=1):
+def cpu_baseline_obj(steps=2, warmup=1):
+    """The CPU path timed on the benchmark configuration itself (same grid, same initial state),
+    plus the x-slab sample of earlier runs as a labelled extra."""
     rate, t, cores = cpu_port_rate(steps, warmup)
-    return {"value": rate, "unit": "DOF-updates/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (NumPy FP64 restatement of the reference step) on Nx={SAMPLE_RES[0]}, "
-                      f"Nu=Nv={SAMPLE_RES[1]}, n={ORDER} ({dof(SAMPLE_RES, ORDER)/1e6:.2f}M DOF), "
+    srate, st, _ = cpu_port_rate(3, 1, res=SAMPLE_RES)
+    return {"value": rate, "unit": "DOF-updates/s", "cores": cores, "kind": "port", "same_config": True,
+            "sample": f"oracle (NumPy FP64 restatement of the reference step) on the full benchmark grid "
+                      f"Nx={RES[0]}, Nu=Nv={RES[1]}, n={ORDER} ({dof(RES, ORDER)/1e6:.2f}M DOF), "
                       f"{steps} steps after {warmup} warm-up, {t:.2f} s/step; BLAS threads = cores, "
-                      "elementwise NumPy single-threaded"}
+                      "elementwise NumPy single-threaded",
+            "slab_sample": {"value": srate, "res": list(SAMPLE_RES), "s_per_step": st}}
 
 
 # ----------------------------------------------------------------------------------------------
@@ -451,18 +457,23 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        # the reference's CPU path (oracle port, all host threads) on rank 0 only
+        # the reference's CPU path (oracle port, all host threads) on rank 0 only, on the benchmark
+        # grid itself: at most 3 timed steps after at most 1 warm-up step (about 13-17 s per step on
+        # 8 host cores), whatever K and W are, so the arm ends within a few minutes
         if rank != 0:
             return 0
-        rate, t, cores = cpu_port_rate(args.steps, args.warmup)
-        sample = (f"oracle (NumPy FP64 restatement of the reference step) on Nx={SAMPLE_RES[0]}, "
-                  f"Nu=Nv={SAMPLE_RES[1]}, n={ORDER}; {t:.2f} s/step")
+        ksteps, kwarm = max(1, min(args.steps, 3)), min(args.warmup, 1)
+        rate, t, cores = cpu_port_rate(ksteps, kwarm)
+        sample = (f"oracle (NumPy FP64 restatement of the reference step) on the full benchmark grid "
+                  f"Nx={RES[0]}, Nu=Nv={RES[1]}, n={ORDER}; {ksteps} timed steps after {kwarm} warm-up, "
+                  f"{t:.2f} s/step")
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "DOF-updates/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "n_gpus": args.gpus, "steps": ksteps, "warmup": kwarm,
                 "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "medium loss-cone config (Nx=32, Nu=Nv=50, n=8), CPU sample "
-                                       f"Nx={SAMPLE_RES[0]}", "dof_sample": dof(SAMPLE_RES, ORDER)},
+                "config": {"workload": "medium loss-cone config: Nx=32, Nu=Nv=50, LGL n=8 "
+                                       "(256x400x400 = 40.96M DOF), j=6, 1e-3 cos kx + 1e-6 noise",
+                           "dof": dof(RES, ORDER), "same_config": True},
                 "cpu_baseline": {"value": rate, "unit": "DOF-updates/s", "cores": cores,
                                  "kind": "port", "sample": sample},
                 "e2e": {"value": rate, "unit": "DOF-updates/s", "h2d_bytes_per_step": 0,
@@ -511,14 +522,18 @@ def main():
                          f"bytes per launch (mean of the 3 stage kinds) = algorithmic x {ratio:.3f}, "
                          f"the DRAM/algorithmic ratio of the ncu capture in {tsrc}",
                          "algorithmic_bytes_per_launch": per_launch,
-                         "kernel": f"stage_frag_kernel<{'double' if prec == 'fp64' else 'float'}>",
+                         "kernel": "stage_frag_kernel<double>" if prec == "fp64" else
+                                   "stage_f32_kernel<kind, background split>",
                          "algorithmic_bytes_per_dof_step": r["bytes_per_dof_step"],
                          "stage_ms": r["stage_ms"], "field_ms": r["field_ms"],
                          "step_effective_gbs": r["dof"] * r["bytes_per_dof_step"] / (ms_step * 1e-3) / 1e9,
                          "peak_source": peak_src},
             "e2e": {"value": dist.sum(r["dof"] * r["steps"] / e2e_s), "unit": "DOF-updates/s",
                     "h2d_bytes_per_step": r["state_bytes"] / r["steps"],
-                    "d2h_bytes_per_step": (r["state_bytes"] + 24 * r["steps"]) / r["steps"]},
+                    "d2h_bytes_per_step": (r["state_bytes"] + 24 * r["steps"]) / r["steps"],
+                    "copies": f"the state copied host->device once and device->host once per "
+                              f"K={r['steps']} steps (a time loop's input and result), plus each "
+                              "step's energy, time and dt; bytes per step = job bytes / K"},
         }
     if rank != 0:
         if world > 1:

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define VL_ABI_VERSION 1
+#define VL_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define VL_API __attribute__((visibility("default")))
@@ -81,8 +81,13 @@ typedef struct vl_config {
     const double *u_nodes;    /* [(nu+2)*n] ghost-inclusive u coordinates (Grid1D.arr) */
     const double *v_nodes;    /* [(nv+2)*n] ghost-inclusive v coordinates */
     const double *wave_numbers; /* [M] */
-    const double *dft_fwd;    /* [nx][n][M] complex, interleaved re/im (Grid1D.spectral_transform) */
-    const double *dft_inv;    /* [M][nx][n] complex, interleaved re/im (Grid1D.grid_phases) */
+    /* The high-order DFT in factored form (complex, interleaved re/im).  The reference's tensor
+     * is their product, T[e, j, m] = dft_phase[e][m] dft_ell[j][m] (Grid1D.spectral_transform,
+     * main/basis.py:204-228), and its inverse phases exp(i k_m x_{e,j}) (Grid1D.grid_phases,
+     * main/grid.py:50) are conj(dft_phase[e][m]) dft_qnode[j][m].                            */
+    const double *dft_ell;    /* [n][M]  Fourier transform of the nodal basis (ell_tilde) */
+    const double *dft_phase;  /* [nx][M] exp(-i k_m mid_e), mid_e the element midpoints */
+    const double *dft_qnode;  /* [n][M]  exp(i k_m (x_{e,j} - mid_e)) */
 } vl_config;
 
 typedef struct vl_ctx vl_ctx;
@@ -116,7 +121,7 @@ VL_API int vl_abi_version(void);
 /* number of elements of one ghost-inclusive state array: (nx+2) n (nu+2) n (nv+2) n */
 VL_API size_t vl_state_elems(const vl_ctx *ctx);
 /* bytes of scratch vl_ssp_rk3_steps needs (caller allocates, 256-B aligned): the moment
- * partials of the stage kernels, then the field solve's mode coefficients and ticket counter */
+ * partials of the stage kernels                                                             */
 VL_API size_t vl_workspace_bytes(const vl_ctx *ctx);
 
 /* ---- hot-path operators ------------------------------------------------------------------ */
@@ -330,10 +335,12 @@ VL_API int vl_closure_apply(void *out, int32_t prec, int32_t nx, int32_t nu, int
  * vl_ssp_rk3_steps minus the workspace: the loop's scratch is a file-scope device array
  * of VL_NOALLOC_SCRATCH_BYTES inside the library (every GPU that loads the library holds it
  * until the process exits).  Problems whose vl_workspace_bytes exceeds that size are rejected
- * with VL_ERR_TOO_LARGE.  The first call on a device looks the array's address up with that
- * device current; make it before any stream capture.  All calls share the array and it keeps
- * the last call's contents (the loop rewrites what it reads; the one word that must start at zero,
- * the field solve's ticket counter, is cleared on the call's stream at its start), so calls
+ * with VL_ERR_TOO_LARGE (the scratch of the problems the kernels accept -- nx n <= 640 -- stays
+ * below 100 KB).  Call it with the context's device current (another device is rejected with
+ * VL_ERR_INVALID).  The first call on a device looks the array's address up with that device
+ * current; make it before any stream capture.  The address is cached for the life of the
+ * process: after a cudaDeviceReset do not call this entry point again on that device.  All calls share the array and it keeps
+ * the last call's contents (the loop writes every entry it reads before reading it), so calls
  * whose kernels overlap on the GPU race on it.  Nothing here calls cudaMalloc or cudaFree.     */
 #define VL_NOALLOC_SCRATCH_BYTES (1u << 20)
 VL_API int vl_ssp_rk3_steps_noalloc(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, double *E,

@@ -1,6 +1,6 @@
 // Host-side check of the shared-memory and tensor-copy geometry of the fragment kernel (n = 8)
-// and of the generic stage kernel's TMA and phased forms, for every compiled order and both
-// precisions: box widths within the
+// and of the generic stage kernel's TMA form, for every compiled order and both precisions: box
+// widths within the
 // tensor-copy limit and 16-byte multiples, every staged array on a 128-byte boundary, the stage
 // ring within the shared memory of one CTA.  Prints one line per failure and "ALL OK" otherwise.
 #include <cstdio>
@@ -33,19 +33,6 @@ void check_tma() {
     expect(G::smem_bytes() <= 227 * 1024, "stage ring fits the shared memory of one CTA", N, es);
 }
 
-template <int N>
-void check_ph() {
-    using G = vl::GenPhGeom<N, float>;
-    expect(G::RS % 4 == 0, "phased row slot is a whole number of 16-byte units", N, 4);
-    // the longest copied run: from the 16-byte boundary up to 3 floats below the left trace through
-    // the right trace, in whole 16-byte units
-    expect(G::RS >= (G::WC + 6) / 4 * 4, "phased row slot holds the run from any 16-byte phase", N, 4);
-    expect(G::IN_B % 128 == 0 && G::XF_B % 128 == 0 && G::BG_B % 128 == 0 && G::UX_B % 128 == 0,
-           "every phased array starts on a 128-byte boundary", N, 4);
-    expect(G::UX_B >= sizeof(double) * (size_t)(N + (N & 1)), "u-node slot holds the even-aligned copy", N, 4);
-    expect(G::smem_bytes() <= 227 * 1024, "phased stage ring fits the shared memory of one CTA", N, 4);
-}
-
 // the order-8 fragment kernel's tile boxes and staged arrays (offsets from the stage start in
 // issue order: tile, f^n tile, x faces, u faces, background tables, u-node speeds)
 template <typename T>
@@ -67,7 +54,6 @@ template <int N>
 void check_order() {
     check_tma<N, double>();
     check_tma<N, float>();
-    check_ph<N>();
 }
 
 int main() {

@@ -1,10 +1,10 @@
 """Generate golden fixtures by running the reference (crewsdw/Vlasov1D2V) on the CPU.
 
-Run in a container that has the reference checkout (default ``/root/reference/main``, override
-with ``VLASOV_REFERENCE_MAIN``)::
+Run in a container that has the reference checkout, with ``VLASOV_REFERENCE_MAIN`` naming its
+``main/`` directory (required; there is no default)::
 
-    python tests/golden/make_golden.py            # all fixtures
-    python tests/golden/make_golden.py basis tiny # a subset
+    VLASOV_REFERENCE_MAIN=<checkout>/main python tests/golden/make_golden.py            # all
+    VLASOV_REFERENCE_MAIN=<checkout>/main python tests/golden/make_golden.py basis tiny # a subset
 
 The reference modules are imported unmodified through ``ref_shim`` (CuPy -> NumPy).  Every
 array written here is produced by reference code; the only inputs built outside the reference
@@ -152,6 +152,23 @@ def gen_small(name, res, order, nsteps, seed):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
+def gen_steps(name, res, order, nsteps, delta_n):
+    """SSP-RK3 steps of the reference from its eigenmode initial state with a large amplitude
+    ``delta_n``: the density perturbation is then a sizeable fraction of the density, so the field
+    (formed from rho - mean(rho)) keeps the relative rounding of rho and the energy history can be
+    held to the 1e-12 bar pointwise."""
+    s = _setup(res, order, delta_n=delta_n)
+    grids, el, f = s["grids"], s["el"], s["f"]
+    out = {"res": np.array(res), "order": np.array(order), "delta_n": np.array(delta_n)}
+    out["f_init"] = _np(f.arr)
+    n0 = f.moment_zero()
+    out["rho_init"] = _np(n0)
+    el.poisson2(charge_density=cp.asarray(n0) - cp.mean(n0), grid=grids.x, basis=s["basis"].b1)
+    out["E_init"] = _np(el.electric_field)
+    _steps(s, nsteps, out)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
 def gen_cfg1(nsteps=200, out_name="cfg1_200", summary=True):
     """Config 1 of the benchmark set: Nx = Nu = Nv = 16, n = 8, loss cone j = 6 times
     (1 + 0.01 cos kx), nsteps SSP-RK3 steps.  Stores the energy/dt/time histories and a
@@ -197,7 +214,9 @@ def gen_linear(res=(4, 6, 5), order=4, nsteps=2):
     n0 = f.moment_zero()
     el.poisson(charge_density=cp.mean(n0) - n0, grid=grids.x, basis=s["basis"].b1)
     out = {"res": np.array(res), "order": order, "f_init": _np(f.arr), "rho_init": _np(n0),
-           "E_dg": _np(el.electric_field), "phi_dg": _np(el.potential)}
+           "E_dg": _np(el.electric_field), "phi_dg": _np(el.potential),
+           "central_flux_operator": _np(el.central_flux_operator),
+           "gradient_operator": _np(el.gradient_operator)}
     st = R.timestep.Stepper(time_order=3, space_order=order, write_time=1.0e9, final_time=1.0e9,
                             linear=True)
     st.adapt_time_step(max_speeds=R.timestep.get_max_speeds(grids, el, s["refs"]),
@@ -235,7 +254,8 @@ def gen_post(res=(3, 3, 4), order=4, seed=5):
 
 
 def main(argv):
-    which = argv or ["basis", "tiny", "small", "n8", "n9", "cfg1", "post", "linear"]
+    which = argv or ["basis", "tiny", "small", "n8", "n9", "tiny_p", "small_p", "n8_p", "n9_p", "cfg1",
+                     "post", "linear"]
     if "basis" in which:
         gen_basis()
     if "tiny" in which:
@@ -246,6 +266,15 @@ def main(argv):
         gen_small("n8", (2, 2, 3), 8, 1, seed=3)
     if "n9" in which:
         gen_small("n9", (2, 2, 2), 9, 1, seed=4)
+    # large-amplitude variants of the four cases: energy bar 1e-12 pointwise
+    if "tiny_p" in which:
+        gen_steps("tiny_p", (3, 4, 5), 3, 3, 0.3)
+    if "small_p" in which:
+        gen_steps("small_p", (4, 6, 5), 4, 4, 0.3)
+    if "n8_p" in which:
+        gen_steps("n8_p", (2, 2, 3), 8, 2, 10.0)
+    if "n9_p" in which:
+        gen_steps("n9_p", (2, 2, 2), 9, 2, 0.3)
     if "cfg1" in which:
         gen_cfg1()
     if "post" in which:

@@ -22,7 +22,8 @@ import types
 
 import numpy as np
 
-REFERENCE_MAIN = os.environ.get("VLASOV_REFERENCE_MAIN", "/root/reference/main")
+# the reference checkout's ``main/`` directory; there is no default: the variable must name it
+REFERENCE_MAIN = os.environ.get("VLASOV_REFERENCE_MAIN", "")
 
 
 class CpArray(np.ndarray):
@@ -119,6 +120,8 @@ def install():
     Returns the imported reference modules as a namespace (basis, grid, elliptic, fluxes,
     timestep, reference).
     """
+    if not REFERENCE_MAIN:
+        raise RuntimeError("set VLASOV_REFERENCE_MAIN to the reference checkout's main/ directory")
     if not os.path.isdir(REFERENCE_MAIN):
         raise FileNotFoundError(REFERENCE_MAIN)
     if not hasattr(np, "math"):
@@ -142,4 +145,4 @@ def install():
 
 
 def available():
-    return os.path.isdir(REFERENCE_MAIN)
+    return bool(REFERENCE_MAIN) and os.path.isdir(REFERENCE_MAIN)

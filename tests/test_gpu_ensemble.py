@@ -74,3 +74,32 @@ def test_ensemble_final_times_and_autotune(cuda, schedule):
     assert probs[0].stepper.steps_counter == 8 and probs[2].stepper.steps_counter == 8
     assert 2 <= probs[1].stepper.steps_counter <= 3
     assert probs[1].stepper.time >= finals[1]
+
+
+@pytest.mark.parametrize("schedule", [(0, 0, 2), (0, 0xFFFFFFFF, 2), (128, 2, 2)],
+                         ids=["by_order", "native_auto", "fused"])
+def test_ensemble_members_against_oracle(cuda, schedule):
+    """Every member (orders 3, 4, 6, 8, 9, each with its own grid and physics) stepped by the
+    ensemble in FP64 against the CPU oracle run from the same initial state: f within 1e-12
+    relative, the energy history within 1e-12 normwise and the clock within 1e-13."""
+    from oracle import vlasov_oracle as vo
+    from vlasov1d2v_b200.ensemble import Ensemble
+
+    probs = [_build(q, "fp64", 3) for q in MEMBERS]
+    refs = []
+    for q, p in zip(MEMBERS, probs):
+        res, n = q["res"], q["order"]
+        c = vo.make_case(*res, n, om_pc=q["om_pc"], k=q["k"])
+        f = p.f.arr.get().copy()
+        rho = vo.moment_zero(f, c)
+        E0, _ = vo.poisson2(rho - np.mean(rho), c)
+        refs.append((f, vo.run(f, c, steps=3, E0=E0)))
+    ens = Ensemble(probs, batch_steps=3)
+    ens.set_schedule(*schedule)
+    ens.run_steps(3)
+    inner = (slice(1, -1), slice(None)) * 3
+    for p, (f, rec) in zip(probs, refs):
+        assert p.stepper.steps_counter == 3
+        assert rel_err(p.f.arr.get()[inner], f[inner]) < 1e-12
+        assert history_err(p.stepper.field_energy, rec.field_energy) < 1e-12
+        np.testing.assert_allclose(p.stepper.time_array, rec.time_array, rtol=1e-13)

@@ -46,23 +46,18 @@ def test_fp32_background_split_against_fp64(cuda):
     assert ferr_split < ferr_plain / 4
 
 
-@pytest.mark.parametrize("form", ["tma", "phased_bulk"])
 @pytest.mark.parametrize("split", [True, False], ids=["background_split", "plain_fp32"])
-def test_fp32_generic_tma_form_in_the_loop(cuda, split, form, monkeypatch):
+def test_fp32_generic_tma_form_in_the_loop(cuda, split, monkeypatch):
     """FP32 order 6 on 16-byte rows, where the generic kernel's TMA form is the stage kernel (with
-    the background split it stages the two background tables as 2-D boxes), and the generic
-    kernel's phased rows filled by bulk copies (VLASOV1D2V_GEN_PHB=1, TMA form off).  6 steps with
-    and without the split match a run on the register-pencil kernel (VLASOV1D2V_STAGE_KERNEL=pencil)."""
+    the background split it stages the two background tables as 2-D boxes).  6 steps with and
+    without the split match a run on the register-pencil kernel (VLASOV1D2V_STAGE_KERNEL=pencil)."""
     from vlasov1d2v_b200 import problem
 
     def run(tma):
-        for var in ("VLASOV1D2V_STAGE_KERNEL", "VLASOV1D2V_GEN_PHB", "VLASOV1D2V_GEN_NO_TMA"):
+        for var in ("VLASOV1D2V_STAGE_KERNEL", "VLASOV1D2V_GEN_NO_TMA"):
             monkeypatch.delenv(var, raising=False)
         if not tma:
             monkeypatch.setenv("VLASOV1D2V_STAGE_KERNEL", "pencil")
-        elif form == "phased_bulk":
-            monkeypatch.setenv("VLASOV1D2V_GEN_PHB", "1")
-            monkeypatch.setenv("VLASOV1D2V_GEN_NO_TMA", "1")
         p = problem.build((4, 4, 6), 6, perturbation="cos", amp=0.01, batch_steps=3, precision="fp32",
                           background_split=split)
         p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, 6)

@@ -40,6 +40,13 @@ def test_grids_bit_identical(name):
     np.testing.assert_array_equal(grids.x.wave_numbers, G["wave_numbers"])
     np.testing.assert_array_equal(grids.x.np_spectral_transform, G["T"])
     np.testing.assert_array_equal(grids.x.np_grid_phases, G["P"])
+    # the factored tables the native field solve reads: T = phase ell exactly as the reference
+    # forms it, and the inverse phases conj(phase) qnode within rounding of the coordinates
+    x = grids.x
+    T = np.transpose(x.np_dft_phase[:, :, None] * x.np_dft_ell.T[None, :, :], (0, 2, 1))
+    np.testing.assert_array_equal(T, G["T"])
+    P = np.conj(x.np_dft_phase).T[:, :, None] * x.np_dft_qnode.T[:, None, :]
+    assert np.max(np.abs(P - G["P"])) < 1e-13
 
 
 @pytest.mark.parametrize("name", SMALL_CASES)

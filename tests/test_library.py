@@ -85,14 +85,14 @@ def test_struct_layout_matches_ctypes(tmp_path):
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "vlasov1d2v.h"\n'
         "int main(void){printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(vl_config),"
-        " offsetof(vl_config, courant), offsetof(vl_config, dft_inv), sizeof(vl_run_state),"
+        " offsetof(vl_config, courant), offsetof(vl_config, dft_qnode), sizeof(vl_run_state),"
         " offsetof(vl_run_state, hist_capacity), offsetof(vl_run_state, dt_hist));return 0;}\n")
     exe = tmp_path / "layout"
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
                                           check=True).stdout.split()]
     C, R = _lib.VlConfig, _lib.VlRunState
-    want = [ctypes.sizeof(C), C.courant.offset, C.dft_inv.offset, ctypes.sizeof(R),
+    want = [ctypes.sizeof(C), C.courant.offset, C.dft_qnode.offset, ctypes.sizeof(R),
             R.hist_capacity.offset, R.dt_hist.offset]
     assert got == want
 

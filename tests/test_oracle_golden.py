@@ -79,6 +79,21 @@ def test_steps(name):
     assert rel_err(f[INNER], G[f"f_step{nst}"]) < 1e-12
 
 
+@pytest.mark.parametrize("name", ("tiny_p", "small_p", "n8_p", "n9_p"))
+def test_steps_large_amplitude(name):
+    """The large-amplitude fixtures: energy of every step within 1e-12 relative, pointwise."""
+    G = golden(name)
+    res = tuple(int(r) for r in G["res"])
+    n = int(G["order"])
+    c = vo.make_case(*res, n)
+    f = G["f_init"].copy()
+    nst = len(G["energy"]) - 1
+    rec = vo.run(f, c, steps=nst, E0=G["E_init"])
+    np.testing.assert_allclose(rec.field_energy, G["energy"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(rec.time_array, G["time"], rtol=1e-14, atol=0)
+    assert rel_err(f[INNER], G[f"f_step{nst}"]) < 1e-12
+
+
 def test_cfg1_first_steps():
     """Config 1 (16^3 elements, n = 8, 1 + 0.01 cos kx): three oracle steps against the first
     entries of the reference's 200-step histories."""
@@ -113,3 +128,26 @@ def test_post_processing_operators():
     ells = [vo.fine_lagrange(c.basis, ax, lim[d]) for d, ax in enumerate((c.x, c.u, c.v))]
     out = vo.interpolate_values(G["state"], *ells, lim)
     assert rel_err(out, G["interp"]) <= 1e-14
+
+
+def test_central_flux_operator_matches_reference():
+    """The DG central-flux Laplacian and gradient map (main/elliptic.py:24-81), assembled here as
+    block linear maps, against the reference's own matrices (probed node by node there)."""
+    from vlasov1d2v_b200.basis import Basis3D
+    from vlasov1d2v_b200.elliptic import central_flux_matrices
+    from vlasov1d2v_b200.grid import Grid1D
+
+    G = golden("linear")
+    res, n = tuple(int(r) for r in G["res"]), int(G["order"])
+    L = 2.0 * np.pi / (0.886 / 10.0)
+    basis = Basis3D(np.array([n] * 3))
+    grid = Grid1D(-L / 2.0, L / 2.0, res[0], basis.b1, spectrum=True)
+    op, grad = central_flux_matrices(grid, basis.b1)
+    ref_op, ref_grad = G["central_flux_operator"], G["gradient_operator"]
+    assert op.shape == ref_op.shape and grad.shape == ref_grad.shape
+    scale = np.max(np.abs(ref_op))
+    assert np.max(np.abs(op - ref_op)) <= 1e-14 * scale
+    assert np.max(np.abs(grad - ref_grad)) <= 1e-14 * np.max(np.abs(ref_grad))
+    # the inverse the solve applies agrees to the conditioning of the bordered system
+    inv, ref_inv = np.linalg.inv(op), np.linalg.inv(ref_op)
+    assert np.max(np.abs(inv - ref_inv)) <= 1e-10 * np.max(np.abs(ref_inv))

@@ -1,4 +1,4 @@
-"""Geometry of the fragment kernel and of the generic stage kernel's TMA and phased forms,
+"""Geometry of the fragment kernel and of the generic stage kernel's TMA form,
 checked on the host (no GPU):
 tensor-copy box widths and alignments, 128-byte staging offsets and shared-memory fit for every
 compiled order and both precisions (tests/geometry/stage_geometry_check.cu, built with nvcc)."""

@@ -16,18 +16,21 @@ from helpers import F_RTOL, INNER, history_err, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _setup():
-    from vlasov1d2v_b200 import problem
+def _setup(res=(3, 4, 5), n=8):
+    from vlasov1d2v_b200 import _lib, problem
     from vlasov1d2v_b200.context import get_context
     from vlasov1d2v_b200.timestep import _BIG_STEPS, _Run, get_max_speeds
 
-    p = problem.build((3, 4, 5), 8, perturbation="cos", amp=0.01)
+    p = problem.build(res, n, perturbation="cos", amp=0.01)
     st = p.stepper
     st.adapt_time_step(get_max_speeds(p.grids, p.elliptic, p.refs), p.grids.x.dx, p.grids.u.dx,
                        p.grids.v.dx)
     ctx = get_context(p.grids, accel=p.refs.electron_acceleration_multiplier,
                       bfield=p.elliptic.magnetic_field, kappa=p.elliptic.poisson_coefficient,
                       courant=st.courant)
+    # the fixed scratch holds this problem with room to spare (the rejection above the capacity
+    # cannot be reached by the grids the kernels accept)
+    assert 0 < ctx.workspace_bytes <= _lib.NOALLOC_SCRATCH_BYTES // 4
     runs = []
     for _ in range(2):
         f = p.f.arr.as_subclass(torch.Tensor).clone()
@@ -40,12 +43,16 @@ def _setup():
 
 def test_noalloc_loop_matches_workspace_loop(cuda):
     ctx, (ra, rb) = _setup()
+    # a second problem of another size and order: its calls leave their own data in the shared
+    # scratch (the moment partials of another grid and kernel layout)
+    ctx2, (_, rc) = _setup((5, 3, 4), 4)
     for call in range(2):   # two calls in a row: the shared scratch carries the last call's data
         ctx.ssp_rk3_steps(ra.f, ra.sa, ra.sb, ra.E, ra.phi, ra.state, 3)
         ctx.ssp_rk3_steps_noalloc(rb.f, rb.sa, rb.sb, rb.E, rb.phi, rb.state, 3)
+        ctx2.ssp_rk3_steps_noalloc(rc.f, rc.sa, rc.sb, rc.E, rc.phi, rc.state, 2)
         torch.cuda.synchronize()
         sa, sb = ra.read_state(), rb.read_state()
-        assert sa.status == 0 and sb.status == 0
+        assert sa.status == 0 and sb.status == 0 and rc.read_state().status == 0
         assert sa.steps == sb.steps == 3 * (call + 1)
         fa = ra.f.cpu().numpy()
         fb = rb.f.cpu().numpy()

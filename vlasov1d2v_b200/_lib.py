@@ -17,7 +17,7 @@ VL_FP64 = 0
 VL_FP32 = 1
 VL_XHALO_GHOST = 0
 VL_XHALO_PERIODIC = 1
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # every symbol include/vlasov1d2v.h declares (checked by the CPU test suite)
 EXPORTED = (
@@ -47,8 +47,8 @@ class VlConfig(ctypes.Structure):
         ("length_x", ctypes.c_double), ("umax", ctypes.c_double), ("vmax", ctypes.c_double),
         ("courant", ctypes.c_double),
         ("up", _c_dbl_p), ("xi", _c_dbl_p), ("xw", _c_dbl_p), ("u_nodes", _c_dbl_p),
-        ("v_nodes", _c_dbl_p), ("wave_numbers", _c_dbl_p), ("dft_fwd", _c_dbl_p),
-        ("dft_inv", _c_dbl_p),
+        ("v_nodes", _c_dbl_p), ("wave_numbers", _c_dbl_p), ("dft_ell", _c_dbl_p),
+        ("dft_phase", _c_dbl_p), ("dft_qnode", _c_dbl_p),
     ]
 
 

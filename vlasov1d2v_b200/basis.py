@@ -199,10 +199,11 @@ class Basis1D:
         der[np.abs(der) < 1.0e-15] = 0
         return der
 
-    def fourier_transform_array(self, midpoints, J, wave_numbers):
-        """High-order DFT tensor T[e, j, m] (``main/basis.py:204-228``): the exact Fourier
-        transform of each element's Legendre modes (spherical Bessel functions) combined with
-        the inverse Vandermonde matrix and the element phase factors.  Host complex128."""
+    def fourier_factors(self, midpoints, J, wave_numbers):
+        """The two factors of the high-order DFT tensor (``main/basis.py:204-228``): the exact
+        Fourier transform of the nodal basis, ell[j, m] (spherical Bessel functions of each
+        Legendre mode combined with the inverse Vandermonde matrix), and the element phases
+        exp(-i k_m mid_e).  Host complex128, [n][M] and [nx][M]."""
         signs = np.sign(wave_numbers)
         signs[np.where(wave_numbers == 0)] = 1.0
         p_tilde = np.array([(signs ** s) * np.exp(-1j * np.pi / 2.0 * s) *
@@ -210,6 +211,12 @@ class Basis1D:
                             for s in range(self.order)])
         ell_tilde = np.matmul(self.vandermonde_inverse.T, p_tilde)
         phase = np.exp(-1j * np.tensordot(midpoints, wave_numbers, axes=0))
+        return ell_tilde, phase
+
+    def fourier_transform_array(self, midpoints, J, wave_numbers):
+        """High-order DFT tensor T[e, j, m] = phase[e, m] ell[j, m] (``main/basis.py:204-228``),
+        host complex128."""
+        ell_tilde, phase = self.fourier_factors(midpoints, J, wave_numbers)
         transform = np.multiply(phase[:, :, None], ell_tilde.T)
         return np.ascontiguousarray(np.transpose(transform, (0, 2, 1)))
 

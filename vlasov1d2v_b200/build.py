@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -42,11 +43,31 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compile every translation unit in parallel (one nvcc per file), then link the library."""
     if not force and not needs_build():
         return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(objdir, os.path.basename(f)[:-3] + ".o") for f in srcs]
+
+    def compile_one(src_obj):
+        src, obj = src_obj
+        cmd = [nvcc(), *ARCH_FLAGS, *COMMON, "-I", INCLUDE, "-I", CSRC, "-c", "-o", obj, src, *extra]
+        if verbose:
+            print(" ".join(cmd))
+        return subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, zip(srcs, objs)))
+    for src, r in zip(srcs, results):
+        if r.stdout or r.stderr:
+            sys.stdout.write(r.stdout)
+            sys.stderr.write(r.stderr)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, f"nvcc {os.path.basename(src)}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *ARCH_FLAGS, *COMMON, "-I", INCLUDE, "-I", CSRC, "-shared", "-o", tmp,
-           *sources(), *extra]
+    cmd = [nvcc(), *ARCH_FLAGS, "-shared", "-o", tmp, *objs]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

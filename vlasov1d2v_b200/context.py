@@ -54,8 +54,9 @@ class NativeContext:
             self._keep.append(a)
             return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
-        fwd = np.ascontiguousarray(x.np_spectral_transform, dtype=np.complex128)
-        inv = np.ascontiguousarray(x.np_grid_phases, dtype=np.complex128)
+        ell = np.ascontiguousarray(x.np_dft_ell, dtype=np.complex128)
+        phase = np.ascontiguousarray(x.np_dft_phase, dtype=np.complex128)
+        qnode = np.ascontiguousarray(x.np_dft_qnode, dtype=np.complex128)
         cfg = _lib.VlConfig()
         cfg.abi_version = _lib.ABI_VERSION
         cfg.precision = _lib.VL_FP64 if precision == "fp64" else _lib.VL_FP32
@@ -80,8 +81,9 @@ class NativeContext:
         cfg.u_nodes = keep(unodes)
         cfg.v_nodes = keep(vnodes)
         cfg.wave_numbers = keep(x.wave_numbers)
-        cfg.dft_fwd = keep(fwd.view(np.float64))
-        cfg.dft_inv = keep(inv.view(np.float64))
+        cfg.dft_ell = keep(ell.view(np.float64))
+        cfg.dft_phase = keep(phase.view(np.float64))
+        cfg.dft_qnode = keep(qnode.view(np.float64))
         self.device = device()
         handle = ctypes.c_void_p()
         with torch.cuda.device(self.device):

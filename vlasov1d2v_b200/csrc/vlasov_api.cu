@@ -21,6 +21,8 @@
 #include "vlasov_stage.cuh"
 #include "vlasov_stage_tma.cuh"
 #include "vlasov_stage_frag.cuh"
+#include "vlasov_stage_f32.cuh"
+#include "vlasov_field.cuh"
 #include "vlasov_stage_gen.cuh"
 
 #include "vlasov_ctx.cuh"
@@ -83,23 +85,18 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// Kernel launch on the caller's stream; inside the RK loop (c->pdl_now) with programmatic
-// dependent launch, so that a kernel's launch and prologue overlap the end of its predecessor
-// (the kernels wait for the predecessor's completion before reading its results).
+// Kernel launch on the caller's stream.
 template <typename... K, typename... A>
 cudaError_t launch(const vl_ctx *c, void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                    A &&...args) {
+    (void)c;
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = c->pdl_now ? 1 : 0;
+    cfg.numAttrs = 0;
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
 }
 
@@ -239,6 +236,35 @@ int gen_bg_map(vl_ctx *c, const float *ptr, CUtensorMap *out) {
     return VL_OK;
 }
 
+// coefficient tables of the FP32 n = 8 kernel (pairs for the packed FMAs), built once per context
+const vl::F32Tables &f32_tables(vl_ctx *c) {
+    if (!c->f32_tables_ready) {
+        constexpr int N = 8;
+        vl::F32Tables &t = c->f32_tables;
+        std::memset(&t, 0, sizeof(t));
+        for (int i = 0; i < N; ++i) {
+            for (int m = 0; m < N; ++m) {
+                const float u = (float)c->up[i * N + m];
+                t.up2[i * N + m] = make_float2(u, u);
+                double p = c->up[i * N + m], q = c->up[i * N + m];
+                if (m == N - 1) p -= c->xi[2 * i + 1];
+                if (m == 0) q += c->xi[2 * i];
+                t.upP[i * N + m] = (float)p;
+                t.upM[i * N + m] = (float)q;
+            }
+            const float l = (float)c->xi[2 * i], r = (float)(-c->xi[2 * i + 1]);
+            t.xl2[i] = make_float2(l, l);
+            t.xr2[i] = make_float2(r, r);
+            const float wu = (float)(c->xw[i] / c->cfg.ju);
+            t.wu2[i] = make_float2(wu, wu);
+            t.wv[i] = c->xw[i] / c->cfg.jv;
+        }
+        for (int i = 0; i < 2 * N; ++i) t.xi[i] = (float)c->xi[i];
+        c->f32_tables_ready = true;
+    }
+    return c->f32_tables;
+}
+
 template <int N, typename T>
 int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
     vl::StageTables<T> tb;
@@ -277,9 +303,35 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                 std::memset(&maps.bg_eu, 0, sizeof(maps.bg_eu));
                 std::memset(&maps.bg_rb, 0, sizeof(maps.bg_rb));
             }
-            return check_launch(launch(c, vl::stage_frag_kernel<T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a, tb,
-                                       maps),
-                                "stage_frag_kernel");
+            if constexpr (sizeof(T) == 4) {
+                // FP32: the packed-FMA kernel, one instantiation per stage kind and background split
+                a.usv = c->d_usv4;
+                const vl::F32Tables &ft = f32_tables(c);
+                const bool bg = a.bg_rb != nullptr;
+                const dim3 blk(G::THREADS);
+                const size_t sm = G::smem_bytes();
+                cudaError_t le;
+                switch (a.kind) {
+                    case vl::KIND_EULER:
+                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_EULER, true>, grid, blk, sm, s, a, ft, maps)
+                                : launch(c, vl::stage_f32_kernel<vl::KIND_EULER, false>, grid, blk, sm, s, a, ft, maps);
+                        break;
+                    case vl::KIND_COMBINE:
+                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_COMBINE, true>, grid, blk, sm, s, a, ft, maps)
+                                : launch(c, vl::stage_f32_kernel<vl::KIND_COMBINE, false>, grid, blk, sm, s, a, ft,
+                                         maps);
+                        break;
+                    default:
+                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_RHS, true>, grid, blk, sm, s, a, ft, maps)
+                                : launch(c, vl::stage_f32_kernel<vl::KIND_RHS, false>, grid, blk, sm, s, a, ft, maps);
+                        break;
+                }
+                return check_launch(le, "stage_f32_kernel");
+            } else {
+                return check_launch(launch(c, vl::stage_frag_kernel<T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
+                                           tb, maps),
+                                    "stage_frag_kernel");
+            }
         }
     }
     if (c->stage_kernel == VL_STAGE_GEN && c->gen_tma) {
@@ -302,29 +354,6 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
         return check_launch(launch(c, vl::stage_gen_tma_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
                                    tb, maps),
                             "stage_gen_tma_kernel");
-    }
-    if constexpr (sizeof(T) == 4) {
-        if (c->stage_kernel == VL_STAGE_GEN && c->gen_phb) {
-            using G = vl::GenPhGeom<N, float>;
-            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
-                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
-                 reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu) |
-                 reinterpret_cast<uintptr_t>(a.u_nodes)) % 16)
-                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
-            return check_launch(launch(c, vl::stage_gen_phb_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s,
-                                       a, tb),
-                                "stage_gen_phb_kernel");
-        }
-        if (c->stage_kernel == VL_STAGE_GEN && c->gen_ph) {
-            using G = vl::GenPhGeom<N, float>;
-            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
-                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
-                 reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu)) % 16)
-                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
-            return check_launch(launch(c, vl::stage_gen_ph_kernel<N>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
-                                       tb),
-                                "stage_gen_ph_kernel");
-        }
     }
     if (c->stage_kernel == VL_STAGE_GEN) {
         using G = vl::GenGeom<N, T>;
@@ -378,28 +407,8 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool ph, bool phb = false) {
+int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
     int blocks = 0;
-    if constexpr (sizeof(T) == 4) {
-        if (gen && phb) {   // FP32: the phased rows by bulk copies
-            using G = vl::GenPhGeom<N, float>;
-            const size_t smem = G::smem_bytes();
-            cudaFuncSetAttribute(vl::stage_gen_phb_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_phb_kernel<N>, G::THREADS,
-                                                              smem) != cudaSuccess)
-                return 1;
-            return blocks > 0 ? blocks : 1;
-        }
-        if (gen && ph) {   // FP32: the phased form
-            using G = vl::GenPhGeom<N, float>;
-            const size_t smem = G::smem_bytes();
-            cudaFuncSetAttribute(vl::stage_gen_ph_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_ph_kernel<N>, G::THREADS,
-                                                              smem) != cudaSuccess)
-                return 1;
-            return blocks > 0 ? blocks : 1;
-        }
-    }
     if (gen && gtma) {
         using G = vl::GenTmaGeom<N, T>;
         const size_t smem = G::smem_bytes();
@@ -422,11 +431,30 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool ph, bool ph
         if (frag) {
             using G = vl::FragGeom<T>;
             const size_t smem = G::smem_bytes();
-            cudaFuncSetAttribute(vl::stage_frag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T>,
-                                                              G::THREADS, smem) != cudaSuccess)
-                return 1;
+            if constexpr (sizeof(T) == 4) {
+                // every instantiation of the FP32 kernel takes the same dynamic shared memory
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_EULER, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_EULER, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_COMBINE, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_COMBINE, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_RHS, true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_RHS, false>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_f32_kernel<vl::KIND_COMBINE, true>,
+                                                                  G::THREADS, smem) != cudaSuccess)
+                    return 1;
+            } else {
+                cudaFuncSetAttribute(vl::stage_frag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem);
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T>,
+                                                                  G::THREADS, smem) != cudaSuccess)
+                    return 1;
+            }
             return blocks > 0 ? blocks : 1;
         }
     }
@@ -461,18 +489,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma, bool ph, bool phb = false) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma, ph, phb);
-        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma, ph, phb);
-        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma, ph, phb);
-        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma, ph, phb);
-        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma, ph, phb);
-        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma, ph, phb);
-        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma, ph, phb);
-        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma, ph, phb);
-        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma, ph, phb);
-        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma, ph, phb);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma);
         default: return 1;
     }
 }
@@ -560,8 +588,9 @@ int moment(const vl_ctx *c, const void *f, double *out, int G, cudaStream_t s) {
 vl::FieldArgs field_args(const vl_ctx *c) {
     vl::FieldArgs a;
     std::memset(&a, 0, sizeof(a));
-    a.fwd = c->d_fwd;
-    a.inv = c->d_inv;
+    a.ell = c->d_ell;
+    a.phase = c->d_phase;
+    a.qnode = c->d_qnode;
     a.k = c->d_k;
     a.xw = c->d_xw;
     a.nx = c->cfg.nx;
@@ -580,28 +609,17 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     return a;
 }
 
-// forward DFT over mode slices, then inverse over node slices (a.scratch carries the
-// coefficients between the two)
+// the whole spectral solve in one CTA (vlasov_field.cuh)
 int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
-    const int nn = c->cfg.nx * c->cfg.n;
-    const int gf = (c->cfg.n_modes + vl::FWD_MODES - 1) / vl::FWD_MODES;
-    const int gi = (nn + vl::INV_NODES - 1) / vl::INV_NODES;
-    const int rc = check_launch(launch(c, vl::field_fwd_kernel, dim3(gf), dim3(vl::FIELD_THREADS), 0, s, a),
-                                "field_fwd_kernel");
-    if (rc) return rc;
-    return check_launch(launch(c, vl::field_inv_kernel, dim3(gi), dim3(vl::FIELD_THREADS), 0, s, a),
-                        "field_inv_kernel");
+    return check_launch(launch(c, vl::field_solve_kernel, dim3(1), dim3(vl::FS_THREADS),
+                               vl::field_solve_smem(c->cfg.n, c->cfg.n_modes), s, a),
+                        "field_solve_kernel");
 }
 
-// byte offset of the field scratch inside a loop workspace (after the moment partials)
+// bytes of the moment partials inside a loop workspace
 size_t partials_bytes(const vl_ctx *c) {
     const int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
     const size_t b = sizeof(double) * (size_t)c->cfg.nx * g * c->cfg.n;
-    return (b + 255) & ~(size_t)255;
-}
-
-size_t field_scratch_bytes(const vl_ctx *c) {
-    const size_t b = sizeof(double) * vl::field_scratch_doubles(c->cfg.n_modes);
     return (b + 255) & ~(size_t)255;
 }
 
@@ -684,7 +702,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if (cfg->n_modes < 1 || cfg->n_modes > vl::FIELD_MAX_MODES)
         return fail(VL_ERR_TOO_LARGE, "number of DFT modes exceeds the field kernel capacity (321)");
     if (!cfg->up || !cfg->xi || !cfg->xw || !cfg->u_nodes || !cfg->v_nodes || !cfg->wave_numbers ||
-        !cfg->dft_fwd || !cfg->dft_inv)
+        !cfg->dft_ell || !cfg->dft_phase || !cfg->dft_qnode)
         return fail(VL_ERR_INVALID, "null table pointer");
     const size_t elems = (size_t)(cfg->nx + 2) * cfg->n * (cfg->nu + 2) * cfg->n *
                          (cfg->nv + 2) * cfg->n;
@@ -696,7 +714,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     vl_ctx *c = new vl_ctx();
     c->cfg = *cfg;
     c->cfg.up = c->cfg.xi = c->cfg.xw = c->cfg.u_nodes = c->cfg.v_nodes = nullptr;
-    c->cfg.wave_numbers = c->cfg.dft_fwd = c->cfg.dft_inv = nullptr;
+    c->cfg.wave_numbers = c->cfg.dft_ell = c->cfg.dft_phase = c->cfg.dft_qnode = nullptr;
     const int n = cfg->n;
     std::memset(c->up, 0, sizeof(c->up));
     std::memset(c->xi, 0, sizeof(c->xi));
@@ -737,14 +755,29 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
                 t[q] = make_float2((float)u, (float)(cfg->accel * (-cfg->bfield * u)));
             }
             if ((rc = upload(&c->d_usv, t.data(), sizeof(float2) * nun))) return cleanup(rc);
+            // the FP32 n = 8 kernel's pairs: {u J_x, u J_x, a (-B u) J_v, a (-B u) J_v}
+            std::vector<float4> t4(nun);
+            for (int q = 0; q < nun; ++q) {
+                const double u = cfg->u_nodes[q];
+                const float ux = (float)(u * cfg->jx), sv = (float)(cfg->accel * (-cfg->bfield * u) * cfg->jv);
+                t4[q] = make_float4(ux, ux, sv, sv);
+            }
+            if ((rc = upload(&c->d_usv4, t4.data(), sizeof(float4) * nun))) return cleanup(rc);
         }
     }
     if ((rc = upload(&c->d_vnodes, cfg->v_nodes, sizeof(double) * (cfg->nv + 2) * n))) return cleanup(rc);
     if ((rc = upload(&c->d_k, cfg->wave_numbers, sizeof(double) * cfg->n_modes))) return cleanup(rc);
     if ((rc = upload(&c->d_xw, cfg->xw, sizeof(double) * n))) return cleanup(rc);
-    const size_t tbytes = sizeof(double2) * (size_t)cfg->nx * n * cfg->n_modes;
-    if ((rc = upload(&c->d_fwd, cfg->dft_fwd, tbytes))) return cleanup(rc);
-    if ((rc = upload(&c->d_inv, cfg->dft_inv, tbytes))) return cleanup(rc);
+    const size_t nm = sizeof(double2) * (size_t)n * cfg->n_modes;
+    if ((rc = upload(&c->d_ell, cfg->dft_ell, nm))) return cleanup(rc);
+    if ((rc = upload(&c->d_phase, cfg->dft_phase, sizeof(double2) * (size_t)cfg->nx * cfg->n_modes)))
+        return cleanup(rc);
+    if ((rc = upload(&c->d_qnode, cfg->dft_qnode, nm))) return cleanup(rc);
+    {
+        const cudaError_t ee = cudaFuncSetAttribute(vl::field_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
+        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaFuncSetAttribute(field_solve_kernel)"));
+    }
     {
         std::vector<double> tabs((size_t)2 * n * n + 2 * n);
         std::memcpy(tabs.data(), c->up, sizeof(double) * n * n);
@@ -760,11 +793,6 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         c->d_err = e0;
         ee = cudaMemset(c->d_err, 0, sizeof(int));
         if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMemset(err)"));
-        const size_t fb = sizeof(double) * vl::field_scratch_doubles(cfg->n_modes);
-        ee = cudaMalloc((void **)&c->d_field, fb);
-        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMalloc(field scratch)"));
-        ee = cudaMemset(c->d_field, 0, fb);
-        if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaMemset(field scratch)"));
     }
     c->use_tma = (cfg->precision == VL_FP64 ? tma_supported<double>(*cfg) : tma_supported<float>(*cfg)) &&
                  encode_fn() != nullptr;
@@ -782,15 +810,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     // FP64 the generic kernel for every other order (its TMA form where the rows allow); in FP32
     // the TMA kernel for n = 4, the generic kernel's TMA form on 16-byte rows and the
     // register-pencil kernel otherwise.
-    // VLASOV1D2V_STAGE_KERNEL=frag|gen|tma|pencil selects one for comparisons
-    // FP32 on the generic kernel's phased form (all rows of one j share a 16-byte phase): opt-in
-    // with VLASOV1D2V_GEN_PH=1; measured within +-16% of the register-pencil kernel (faster at
-    // n = 7, 9, slower at n = 5, 6), so the pencil kernel stays the FP32 default
-    const bool ph_ok = ((size_t)(cfg->nu + 2) * n * (size_t)(cfg->nv + 2) * n) % 4 == 0;
-    {
-        const char *env = getenv("VLASOV1D2V_GEN_PH");
-        c->gen_ph = cfg->precision == VL_FP32 && ph_ok && env && env[0] == '1';
-    }
+    // VLASOV1D2V_STAGE_KERNEL=frag|gen|pencil selects one of the forms that apply, for comparisons
     // FP32 on the generic kernel's TMA form where the rows are 16-byte multiples ((nv+2) n a
     // multiple of 4), orders other than 4 and 8; VLASOV1D2V_GEN_NO_TMA=1 switches it off
     const bool no_gen_tma = [] {
@@ -799,16 +819,10 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     }();
     const bool gen_tma32 = cfg->precision == VL_FP32 && ((size_t)(cfg->nv + 2) * n) % 4 == 0 && !no_gen_tma &&
                            encode_fn() != nullptr;
-    // FP32 rows that are not 16-byte multiples but share a phase per j (as the phased form):
-    // the phased rows filled by bulk copies on mbarriers, opt-in with VLASOV1D2V_GEN_PHB=1
-    {
-        const char *env = getenv("VLASOV1D2V_GEN_PHB");
-        c->gen_phb = cfg->precision == VL_FP32 && ph_ok && !gen_tma32 && env && env[0] == '1';
-    }
     c->stage_kernel = c->use_frag                                  ? VL_STAGE_FRAG
                       : cfg->precision == VL_FP64                  ? VL_STAGE_GEN
                       : c->use_tma                                 ? VL_STAGE_TMA
-                      : (c->gen_ph || gen_tma32 || c->gen_phb)     ? VL_STAGE_GEN
+                      : gen_tma32                                  ? VL_STAGE_GEN
                                                                    : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
@@ -816,7 +830,6 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
             const std::string k(env);
             if (k == "gen") c->stage_kernel = VL_STAGE_GEN;
             else if (k == "pencil") c->stage_kernel = VL_STAGE_PENCIL;
-            else if (k == "tma" && c->use_tma) c->stage_kernel = VL_STAGE_TMA;
             else if (k == "frag" && c->use_frag) c->stage_kernel = VL_STAGE_FRAG;
         }
         c->use_frag = c->stage_kernel == VL_STAGE_FRAG;
@@ -826,12 +839,9 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even), FP32 as above
     c->gen_tma = gen && (cfg->precision == VL_FP64 ? ((size_t)(cfg->nv + 2) * n) % 2 == 0 : gen_tma32) &&
                  encode_fn() != nullptr && !no_gen_tma;
-    c->gen_phb = c->gen_phb && gen && !c->gen_tma;
-    c->gen_ph = c->gen_ph && gen && !c->gen_tma && !c->gen_phb;
     const int occ = cfg->precision == VL_FP64
-                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma, false)
-                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma, c->gen_ph,
-                                                 c->gen_phb);
+                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma)
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double
@@ -858,13 +868,14 @@ int vl_ctx_destroy(vl_ctx *c) {
     if (c == nullptr) return VL_OK;
     cudaFree(c->d_unodes);
     cudaFree(c->d_usv);
+    cudaFree(c->d_usv4);
     cudaFree(c->d_vnodes);
     cudaFree(c->d_k);
     cudaFree(c->d_xw);
-    cudaFree(c->d_fwd);
-    cudaFree(c->d_inv);
+    cudaFree(c->d_ell);
+    cudaFree(c->d_phase);
+    cudaFree(c->d_qnode);
     cudaFree(c->d_tables);
-    cudaFree(c->d_field);
     cudaFree(c->d_moment);
     cudaFree(c->d_err);
     delete c;
@@ -879,7 +890,7 @@ size_t vl_state_elems(const vl_ctx *c) {
 
 size_t vl_workspace_bytes(const vl_ctx *c) {
     if (c == nullptr) return 0;
-    return partials_bytes(c) + field_scratch_bytes(c);
+    return partials_bytes(c);
 }
 
 int vl_rhs(vl_ctx *c, const void *f, const double *E, void *out, int xhalo, void *stream) {
@@ -927,7 +938,6 @@ int vl_poisson(vl_ctx *c, const double *charge, double *E, double *phi, void *st
     a.charge_in = charge;
     a.E = E;
     a.phi = phi;
-    a.scratch = c->d_field;
     return field(c, a, as_stream(stream));
 }
 
@@ -1023,16 +1033,12 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     if (nsteps < 0) return fail(VL_ERR_INVALID, "nsteps < 0");
     cudaStream_t s = as_stream(stream);
     double *partials = static_cast<double *>(workspace);
-    double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) + partials_bytes(c));
     const int G = c->stage_grid_g;
     int rc;
-    // the field solve's ticket counter starts at zero (the last CTA of each record resets it)
-    VL_CUDA(cudaMemsetAsync(fscratch + 4 * (size_t)c->cfg.n_modes, 0, sizeof(int), s));
     // moment partials of f^n for the first step's field solve
     if ((rc = moment(c, f, partials, c->moment_grid_g, s))) return rc;
     vl::FieldArgs fa = field_args(c);
     fa.partials = partials;
-    fa.scratch = fscratch;
     fa.G = c->moment_grid_g;
     fa.E = E;
     fa.state = state;
@@ -1043,13 +1049,6 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
     st.err = &state->status;   // bounded-wait timeouts are reported in the loop state
     st.xhalo = VL_XHALO_PERIODIC;
     st.partials = partials;
-    // field and stage launches of the loop overlap their predecessors (programmatic dependent
-    // launch); restored on every return
-    struct PdlScope {
-        vl_ctx *c;
-        explicit PdlScope(vl_ctx *cc) : c(cc) { c->pdl_now = c->use_pdl; }
-        ~PdlScope() { c->pdl_now = false; }
-    } pdl_scope(c);
     for (int it = 0; it < nsteps; ++it) {
         // stage 0: E(f^n); s0 = f + dt R(f)  (main/timestep.py:153-163)
         fa.mode = vl::FIELD_PROMOTE;

@@ -10,6 +10,7 @@
 
 #include "vlasov1d2v.h"
 #include "vlasov_kernels.cuh"
+#include "vlasov_stage_f32.cuh"
 
 enum vl_stage_kernel { VL_STAGE_PENCIL = 0, VL_STAGE_TMA = 1, VL_STAGE_FRAG = 2, VL_STAGE_GEN = 3 };
 
@@ -25,26 +26,25 @@ struct vl_ctx {
     double qw[vl::NMAX * vl::NMAX];
     double *d_unodes = nullptr;
     void *d_usv = nullptr;        // per u node (u, a (-B u)), double2 or float2
+    float4 *d_usv4 = nullptr;     // FP32: per u node {u J_x, u J_x, a (-B u) J_v, a (-B u) J_v}
     double *d_vnodes = nullptr;
     double *d_k = nullptr;
     double *d_xw = nullptr;
-    double2 *d_fwd = nullptr;
-    double2 *d_inv = nullptr;
+    double2 *d_ell = nullptr;     // [n][M]  DFT factors (vl_config dft_ell / dft_phase / dft_qnode)
+    double2 *d_phase = nullptr;   // [nx][M]
+    double2 *d_qnode = nullptr;   // [n][M]
     double *d_tables = nullptr;   // up [n n], xi [n 2], qw [n n]
-    double *d_field = nullptr;    // field scratch of vl_poisson (mode coefficients)
     double *d_moment = nullptr;   // moment partials of vl_moment [nx][moment_grid_g][n]
     int *d_err = nullptr;         // device error word of operators run without a loop state
     bool use_tma = false;         // stage kernel: TMA-pipelined form (aligned orders)
     bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
     int stage_kernel = VL_STAGE_GEN;   // which stage kernel the launches use (vl_stage_kernel)
     bool gen_tma = false;         // generic stage kernel in its TMA form (FP64, aligned rows)
-    bool gen_ph = false;          // generic stage kernel in its phased form (FP32)
-    bool gen_phb = false;         // the phased rows filled by bulk copies on mbarriers (FP32)
-    bool use_pdl = false;         // loop launches with programmatic dependent launch
-    bool pdl_now = false;         // set while vl_ssp_rk3_steps issues its launches
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
     const float *bg_eu = nullptr;
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
+    vl::F32Tables f32_tables;       // FP32 n = 8 kernel's coefficient pairs (built on first use)
+    bool f32_tables_ready = false;
 };
 
 

@@ -22,33 +22,44 @@ struct DgArgs {
     const double *inv;      // [(nn + 1)^2] inverse of the bordered central-flux operator
     const double *mass;     // [n][n]
     const double *grad;     // [nn][nn] gradient operator G[q][p]
-    const double2 *fwd;     // [nn][M]
-    const double2 *ph;      // [M][nn]
+    const double2 *ell;     // [n][M]  DFT factors of the context: T[e, j, m] = phase[e, m] ell[j, m]
+    const double2 *phase;   // [nx][M]
+    const double2 *qnode;   // [n][M]  exp(i k_m x_{e,j}) = conj(phase[e, m]) qnode[j, m]
     double *E;              // [(nx + 2) n]
     double *phi;            // [nn] or null
     int nx, n, M, anti_alias;
     double kappa, J, dx, length;
 };
 
-// v <- Re sum_m c_m P[m][p], c_m = (sum_p v_p T[p][m]) dx / L   (grid.fourier_basis + sum_fourier)
+// v <- Re sum_m c_m exp(i k_m x_p), c_m = (sum_p v_p T[p][m]) dx / L   (grid.fourier_basis +
+// sum_fourier), with the DFT in its factored form
 __device__ void dft_filter(double *v, double2 *coef, const DgArgs &a) {
-    const int nn = a.nx * a.n;
-    for (int m = threadIdx.x; m < a.M; m += blockDim.x) {
+    const int nn = a.nx * a.n, n = a.n, M = a.M;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
         double cr = 0.0, ci = 0.0;
-        for (int p = 0; p < nn; ++p) {
-            const double2 t = a.fwd[(size_t)p * a.M + m];
-            cr = fma(v[p], t.x, cr);
-            ci = fma(v[p], t.y, ci);
+        for (int e = 0; e < a.nx; ++e) {
+            double sr = 0.0, si = 0.0;
+            for (int j = 0; j < n; ++j) {
+                const double2 l = a.ell[(size_t)j * M + m];
+                sr = fma(v[e * n + j], l.x, sr);
+                si = fma(v[e * n + j], l.y, si);
+            }
+            const double2 ph = a.phase[(size_t)e * M + m];
+            cr = fma(ph.x, sr, fma(-ph.y, si, cr));
+            ci = fma(ph.x, si, fma(ph.y, sr, ci));
         }
         coef[m] = make_double2((cr * a.dx) / a.length, (ci * a.dx) / a.length);
     }
     __syncthreads();
     for (int p = threadIdx.x; p < nn; p += blockDim.x) {
+        const int e = p / n, j = p - e * n;
         double s = 0.0;
-        for (int m = 0; m < a.M; ++m) {
-            const double2 q = a.ph[(size_t)m * nn + p];
-            s = fma(coef[m].x, q.x, s);
-            s = fma(-coef[m].y, q.y, s);
+        for (int m = 0; m < M; ++m) {
+            // Re(c conj(h) q) with conj(h) q = exp(i k x_p)
+            const double2 h = a.phase[(size_t)e * M + m], q = a.qnode[(size_t)j * M + m];
+            const double pr = h.x * q.x + h.y * q.y, pi = h.x * q.y - h.y * q.x;
+            s = fma(coef[m].x, pr, s);
+            s = fma(-coef[m].y, pi, s);
         }
         v[p] = s;   // each thread rewrites only its own entries, read by nobody else meanwhile
     }
@@ -138,8 +149,9 @@ VL_API int vl_poisson_dg(vl_ctx *c, const double *charge, const double *inv_op, 
     a.inv = inv_op;
     a.mass = mass;
     a.grad = grad_op;
-    a.fwd = c->d_fwd;
-    a.ph = c->d_inv;
+    a.ell = c->d_ell;
+    a.phase = c->d_phase;
+    a.qnode = c->d_qnode;
     a.E = E;
     a.phi = phi;
     a.nx = c->cfg.nx;

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "vlasov_ctx.cuh"
+#include "vlasov_field.cuh"
 #include "vlasov_stage.cuh"
 
 namespace vl {
@@ -197,24 +198,9 @@ ens_order_kernel(const EnsMember *__restrict__ members, const int *__restrict__ 
     }
 }
 
-// field solves of all members: blockIdx.y = member, blockIdx.x = mode / node chunk
-__global__ void __launch_bounds__(FIELD_THREADS) ens_field_fwd_kernel(const FieldArgs *__restrict__ fa) {
-    const FieldArgs &a = fa[blockIdx.y];
-    if ((int)blockIdx.x * FWD_MODES >= a.M) return;
-    field_fwd_body(a, blockIdx.x);
-}
-
-__global__ void __launch_bounds__(FIELD_THREADS) ens_field_inv_kernel(const FieldArgs *__restrict__ fa) {
-    const FieldArgs &a = fa[blockIdx.y];
-    const int nb = (a.nx * a.n + INV_NODES - 1) / INV_NODES;
-    if ((int)blockIdx.x >= nb) return;
-    field_inv_body(a, blockIdx.x, nb);
-}
-
-// clear every member's field ticket counter (start of a call)
-__global__ void ens_reset_kernel(const FieldArgs *__restrict__ fa, int count) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < count) *reinterpret_cast<int *>(fa[i].scratch + 4 * (size_t)fa[i].M) = 0;
+// field solves of all members: one CTA per member (vlasov_field.cuh)
+__global__ void __launch_bounds__(FS_THREADS) ens_field_kernel(const FieldArgs *__restrict__ fa) {
+    field_solve_body(fa[blockIdx.x]);
 }
 
 }  // namespace vl
@@ -250,7 +236,7 @@ struct vl_ens {
     vl::FieldArgs *d_field[3] = {nullptr, nullptr, nullptr};
     int *d_cta_items = nullptr;
     vl::EnsItem *d_items = nullptr;
-    int max_fwd = 1, max_inv = 1;
+    size_t field_smem = 0;   // dynamic shared memory of the field kernel: the largest member's
     bool dirty = true;
 };
 
@@ -274,11 +260,6 @@ int tiles_of(const vl_ctx *c) {
 
 size_t partial_bytes(const vl_ctx *c, int G) {
     const size_t b = sizeof(double) * (size_t)c->cfg.nx * G * c->cfg.n;
-    return (b + 255) & ~(size_t)255;
-}
-
-size_t field_bytes(const vl_ctx *c) {
-    const size_t b = sizeof(double) * vl::field_scratch_doubles(c->cfg.n_modes);
     return (b + 255) & ~(size_t)255;
 }
 
@@ -404,12 +385,9 @@ int stage(vl_ens *E, int st, cudaStream_t s) {
 
 int field(vl_ens *E, int kind, cudaStream_t s) {
     const int count = (int)E->ctx.size();
-    vl::ens_field_fwd_kernel<<<dim3(E->max_fwd, count), vl::FIELD_THREADS, 0, s>>>(E->d_field[kind]);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_fwd_kernel: ") + cudaGetErrorString(e));
-    vl::ens_field_inv_kernel<<<dim3(E->max_inv, count), vl::FIELD_THREADS, 0, s>>>(E->d_field[kind]);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_inv_kernel: ") + cudaGetErrorString(e));
+    vl::ens_field_kernel<<<count, vl::FS_THREADS, E->field_smem, s>>>(E->d_field[kind]);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_kernel: ") + cudaGetErrorString(e));
     return VL_OK;
 }
 
@@ -472,7 +450,7 @@ int commit(vl_ens *E) {
     // item costs: tiles per item x n^3 (DOFs per tile ~ 32 n^2, contraction length n); items of
     // order n go to list n (by-order schedule) or all to list 0
     std::vector<CostItem> items[vl::NMAX + 1];
-    E->max_fwd = E->max_inv = 1;
+    E->field_smem = 0;
     for (int i = 0; i < count; ++i) {
         const vl_ctx *c = E->ctx[i];
         const int G = E->G[i];
@@ -487,8 +465,7 @@ int commit(vl_ens *E) {
             }
         E->members[i].G = G;
         for (int k = 0; k < 3; ++k) E->field[k][i].G = G;
-        E->max_fwd = std::max(E->max_fwd, (c->cfg.n_modes + vl::FWD_MODES - 1) / vl::FWD_MODES);
-        E->max_inv = std::max(E->max_inv, (c->cfg.nx * c->cfg.n + vl::INV_NODES - 1) / vl::INV_NODES);
+        E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes));
     }
     std::vector<int> offs;
     std::vector<vl::EnsItem> flat;
@@ -579,6 +556,8 @@ VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out) {
             cudaFuncSetAttribute(t == 64 ? vl::ens_stage_kernel<float, 64> : vl::ens_stage_kernel<float, 128>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
+    cudaFuncSetAttribute(vl::ens_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
     *out = E;
     return VL_OK;
 }
@@ -599,7 +578,7 @@ VL_API int vl_ens_destroy(vl_ens *E) {
 VL_API size_t vl_ens_workspace_bytes(const vl_ens *E, int32_t i) {
     if (!E || i < 0 || i >= (int)E->ctx.size()) return 0;
     const vl_ctx *c = E->ctx[i];
-    return partial_bytes(c, tiles_of(c)) + field_bytes(c);   // partials for any schedule
+    return partial_bytes(c, tiles_of(c));   // partials for any schedule
 }
 
 VL_API int vl_ens_bind(vl_ens *E, int32_t i, void *f, void *sa, void *sb, double *Ef, double *phi,
@@ -633,8 +612,6 @@ VL_API int vl_ens_bind(vl_ens *E, int32_t i, void *f, void *sa, void *sb, double
     a.jx = c->cfg.jx;
     a.ju = c->cfg.ju;
     a.jv = c->cfg.jv;
-    double *fscratch = reinterpret_cast<double *>(static_cast<char *>(workspace) +
-                                                  partial_bytes(c, tiles_of(c)));
     const int modes[3] = {vl::FIELD_PROMOTE, vl::FIELD_REQUIRE_ACTIVE,
                           vl::FIELD_REQUIRE_ACTIVE | vl::FIELD_RECORD};
     for (int k = 0; k < 3; ++k) {
@@ -646,9 +623,9 @@ VL_API int vl_ens_bind(vl_ens *E, int32_t i, void *f, void *sa, void *sb, double
         fa.phi = (k == 2) ? phi : nullptr;
         fa.state = state;
         fa.mode = modes[k];
-        fa.scratch = fscratch;
-        fa.fwd = c->d_fwd;
-        fa.inv = c->d_inv;
+        fa.ell = c->d_ell;
+        fa.phase = c->d_phase;
+        fa.qnode = c->d_qnode;
         fa.k = c->d_k;
         fa.xw = c->d_xw;
         fa.nx = c->cfg.nx;
@@ -790,8 +767,6 @@ VL_API int vl_ens_steps(vl_ens *E, int32_t nsteps, void *stream) {
     int rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int count = (int)E->ctx.size();
-    vl::ens_reset_kernel<<<(count + 127) / 128, 128, 0, s>>>(E->d_field[0], count);
-    VL_ECUDA(cudaGetLastError());
     // density partials of every member's f^n for the first field solve
     for (int i = 0; i < count; ++i)
         if ((rc = vl_internal_moment(E->ctx[i], E->members[i].f, E->members[i].a.partials, E->G[i], s)))

@@ -70,15 +70,6 @@ struct StageArgs {
     const float *bg_eu;
 };
 
-// Programmatic dependent launch (opt-in, VLASOV1D2V_PDL=1).  Inside the RK loop every kernel is
-// then launched so that it may
-// start while its predecessor on the stream finishes; before reading anything the predecessor
-// writes it waits for that grid's completion (a no-op for a plain launch), and only then lets its
-// own dependents launch.  Every kernel waits before any exit, so the completion of a kernel
-// implies the completion of all earlier ones, and a kernel that has started may read data
-// written two or more launches back (loop state, the previous stage's output).
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // SSP-RK combination stage c0 f^n + c1 s + (c2 dt) r with c0 + c1 = 1 (main/timestep.py:157-163,
 // :174-182).  FP64 evaluates the reference's expression as written; FP32 evaluates
@@ -163,7 +154,6 @@ constexpr int MOMENT_CTAS_PER_SM = 4;
 
 template <int N, typename T>
 __global__ void __launch_bounds__(MOMENT_THREADS, MOMENT_CTAS_PER_SM) moment_kernel(const MomentArgs a) {
-    pdl_wait();
     const T *__restrict__ f = static_cast<const T *>(a.f);
     constexpr int CT = (MOMENT_THREADS / N) * N;   // column threads (stride keeps k fixed)
     const int g = blockIdx.x, Gn = gridDim.x, e = blockIdx.y;
@@ -214,14 +204,7 @@ static __global__ void moment_reduce_kernel(const double *__restrict__ partials,
 }
 
 // ----------------------------------------------------------------------------------------------
-// field solve: two multi-CTA kernels
-//   field_fwd_kernel  every CTA forms the charge kappa (mean rho - rho) from the moment partials
-//                     (fixed summation order), then a slice of FWD_MODES modes:
-//                     c_m = (sum_{e,j} rhs T[e,j,m]) dx / L, Ehat_m = -c_m/(i k_m),
-//                     phihat_m = -c_m / k_m^2 (k = 0 mode dropped) -> scratch
-//   field_inv_kernel  a slice of INV_NODES nodes: E = Re sum_m Ehat_m P[m,e,j], phi likewise,
-//                     periodic ghost rows.  After stage 2 the last CTA to finish (ticket
-//                     counter) records the energy, adapts dt and updates the loop state.
+// field solve (the kernel itself is vlasov_field.cuh): arguments, loop gating, reductions
 // ----------------------------------------------------------------------------------------------
 enum FieldMode : int {
     FIELD_REQUIRE_ACTIVE = 1,  // return if !state->active
@@ -237,23 +220,18 @@ struct FieldArgs {
     double *phi;              // [nx n] or null
     vl_run_state *state;      // or null
     int mode;
-    double *scratch;          // [4 M] Ehat | phihat (complex, interleaved), then an int counter
-    const double2 *fwd;       // [nx n][M]
-    const double2 *inv;       // [M][nx n]
+    const double2 *ell;       // [n][M]   T[e, j, m] = phase[e, m] ell[j, m]
+    const double2 *phase;     // [nx][M]  exp(-i k_m mid_e)
+    const double2 *qnode;     // [n][M]   exp(i k_m x_{e,j}) = conj(phase[e, m]) qnode[j, m]
     const double *k;          // [M]
     const double *xw;         // [n]
     int nx, n, M;
     double kappa, dx, length, accel, bfield, umax, vmax, du, dv, courant;
 };
 
-constexpr int FIELD_THREADS = 1024;
-constexpr int FWD_MODES = 16;                  // modes per forward CTA
-constexpr int INV_NODES = 16;                  // nodes per inverse CTA
-constexpr int FIELD_PARTS = FIELD_THREADS / 16;   // partial sums per mode / node
+constexpr int FIELD_THREADS = 1024;            // threads of the single-CTA field and scalar kernels
 constexpr int FIELD_MAX_NODES = 64 * NMAX;    // nx * n capacity of the shared buffers
 constexpr int FIELD_MAX_MODES = 2 * 160 + 1;  // M capacity
-
-__host__ __device__ constexpr size_t field_scratch_doubles(int M) { return 4 * (size_t)M + 8; }
 
 __device__ __forceinline__ double block_sum_dd(double v, double c, dd *scratch) {
     return block_sum_dd_rt(v, c, scratch);
@@ -284,207 +262,6 @@ __device__ __forceinline__ bool field_gate(const FieldArgs &a, bool first_cta) {
     }
     if (a.mode & FIELD_REQUIRE_ACTIVE) return st->active != 0;
     return true;
-}
-
-// CTA bx of the forward transform of one problem (modes 16 bx .. 16 bx + 15)
-__device__ __forceinline__ void field_fwd_body(const FieldArgs &a, int bx) {
-    __shared__ double s_rhs[FIELD_MAX_NODES];
-    __shared__ double s_cr[FIELD_PARTS][FWD_MODES + 1], s_ci[FIELD_PARTS][FWD_MODES + 1];
-    __shared__ dd s_red[FIELD_THREADS / 32];
-    static_assert(FIELD_PARTS * FWD_MODES == FIELD_THREADS && FIELD_PARTS == 64 &&
-                      FWD_MODES <= FIELD_THREADS / 32, "forward thread layout");
-    if (!field_gate(a, bx == 0)) return;
-    const int tid = threadIdx.x;
-    const int nn = a.nx * a.n;
-    const int M = a.M;
-    if (a.charge_in != nullptr) {
-        for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * a.charge_in[p];
-        __syncthreads();
-    } else {
-        double loc = 0.0, locc = 0.0;
-        for (int p = tid; p < nn; p += blockDim.x) {
-            const int e = p / a.n, i = p - (p / a.n) * a.n;
-            dd sacc = {0.0, 0.0};
-            for (int gg = 0; gg < a.G; ++gg)
-                sacc = dd_add(sacc, dd{a.partials[((size_t)e * a.G + gg) * a.n + i], 0.0});
-            const double rho = sacc.hi + sacc.lo;
-            s_rhs[p] = rho;
-            const double t = loc + rho;
-            locc += (fabs(loc) >= fabs(rho)) ? ((loc - t) + rho) : ((rho - t) + loc);
-            loc = t;
-        }
-        const double total = block_sum_dd(loc, locc, s_red);
-        const double mean = total / (double)nn;
-        __syncthreads();
-        for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * (mean - s_rhs[p]);
-        __syncthreads();
-    }
-    // this CTA's modes: thread (mode slot ml, part) sums nodes p = part, part + PARTS, ...
-    const int ml = tid % FWD_MODES, part = tid / FWD_MODES;
-    const int m = bx * FWD_MODES + ml;
-    double cr = 0.0, ci = 0.0;
-    if (m < M) {
-#pragma unroll 4
-        for (int p = part; p < nn; p += FIELD_PARTS) {
-            const double2 t = a.fwd[(size_t)p * M + m];
-            const double r = s_rhs[p];
-            cr = fma(r, t.x, cr);
-            ci = fma(r, t.y, ci);
-        }
-    }
-    s_cr[part][ml] = cr;
-    s_ci[part][ml] = ci;
-    __syncthreads();
-    // warp w folds the 64 partial sums of mode slot w
-    const int w = tid >> 5, lane = tid & 31;
-    const int mw = bx * FWD_MODES + w;
-    if (w < FWD_MODES && mw < M) {
-        double sr = s_cr[lane][w] + s_cr[lane + 32][w];
-        double si = s_ci[lane][w] + s_ci[lane + 32][w];
-        for (int off = 16; off > 0; off >>= 1) {
-            sr += __shfl_down_sync(0xffffffffu, sr, off);
-            si += __shfl_down_sync(0xffffffffu, si, off);
-        }
-        if (lane != 0) return;
-        const int m = mw;
-        sr = (sr * a.dx) / a.length;
-        si = (si * a.dx) / a.length;
-        const double km = a.k[m];
-        double2 Eh, Ph;
-        if (km == 0.0) {
-            // CuPy's complex division by zero gives nan+nanj, which nan_to_num turns into 0
-            // (main/elliptic.py:124-128): the mean mode is dropped.
-            Eh = make_double2(0.0, 0.0);
-            Ph = make_double2(0.0, 0.0);
-        } else {
-            // -(c / (1j k)) = (-c_i / k) + 1j (c_r / k);  -(c / k^2)
-            Eh = make_double2(-(si / km), sr / km);
-            const double k2 = km * km;
-            Ph = make_double2(-(sr / k2), -(si / k2));
-        }
-        double2 *sc = reinterpret_cast<double2 *>(a.scratch);
-        sc[m] = Eh;
-        sc[M + m] = Ph;
-    }
-}
-
-static __global__ void __launch_bounds__(FIELD_THREADS) field_fwd_kernel(const FieldArgs a) {
-    pdl_wait();
-    pdl_trigger();
-    field_fwd_body(a, blockIdx.x);
-}
-
-// CTA bx of nblocks of the inverse transform of one problem (nodes 16 bx .. 16 bx + 15); the
-// last of the nblocks CTAs to finish does the loop bookkeeping
-__device__ __forceinline__ void field_inv_body(const FieldArgs &a, int bx, int nblocks) {
-    __shared__ double2 s_E[FIELD_MAX_MODES];
-    __shared__ double2 s_P[FIELD_MAX_MODES];
-    __shared__ double s_er[FIELD_PARTS][INV_NODES + 1], s_pr[FIELD_PARTS][INV_NODES + 1];
-    __shared__ dd s_red[FIELD_THREADS / 32];
-    __shared__ double s_max[FIELD_THREADS / 32];
-    __shared__ int s_last;
-    static_assert(FIELD_PARTS * INV_NODES == FIELD_THREADS && FIELD_PARTS == 64 &&
-                      INV_NODES <= FIELD_THREADS / 32, "inverse thread layout");
-    vl_run_state *st = a.state;
-    if (st != nullptr && (a.mode & (FIELD_REQUIRE_ACTIVE | FIELD_PROMOTE)) && st->active == 0) return;
-    const int tid = threadIdx.x;
-    const int nn = a.nx * a.n;
-    const int M = a.M;
-    const double2 *sc = reinterpret_cast<const double2 *>(a.scratch);
-    for (int m = tid; m < M; m += blockDim.x) {
-        s_E[m] = sc[m];
-        s_P[m] = sc[M + m];
-    }
-    __syncthreads();
-    const int nl = tid % INV_NODES, part = tid / INV_NODES;
-    const int p = bx * INV_NODES + nl;
-    double er = 0.0, pr = 0.0;
-    if (p < nn) {
-#pragma unroll 4
-        for (int m = part; m < M; m += FIELD_PARTS) {
-            const double2 ph = a.inv[(size_t)m * nn + p];
-            const double2 eh = s_E[m];
-            const double2 qh = s_P[m];
-            er = fma(eh.x, ph.x, er);
-            er = fma(-eh.y, ph.y, er);
-            pr = fma(qh.x, ph.x, pr);
-            pr = fma(-qh.y, ph.y, pr);
-        }
-    }
-    s_er[part][nl] = er;
-    s_pr[part][nl] = pr;
-    __syncthreads();
-    // warp w folds the 64 partial sums of node slot w
-    const int w = tid >> 5, lane = tid & 31;
-    const int pw = bx * INV_NODES + w;
-    if (w < INV_NODES && pw < nn) {
-        double se = s_er[lane][w] + s_er[lane + 32][w];
-        double sp = s_pr[lane][w] + s_pr[lane + 32][w];
-        for (int off = 16; off > 0; off >>= 1) {
-            se += __shfl_down_sync(0xffffffffu, se, off);
-            sp += __shfl_down_sync(0xffffffffu, sp, off);
-        }
-        if (lane == 0) {
-            a.E[a.n + pw] = se;
-            if (pw >= nn - a.n) a.E[pw - (nn - a.n)] = se;   // E[0] = E[-2]
-            if (pw < a.n) a.E[nn + a.n + pw] = se;           // E[-1] = E[1]
-            if (a.phi != nullptr) a.phi[pw] = sp;
-            if (st != nullptr && !isfinite(se)) atomicOr(&st->status, 1);
-        }
-    }
-    if (st == nullptr || !(a.mode & FIELD_RECORD)) return;
-    // ---- last CTA: energy, dt, loop bookkeeping (main/timestep.py:98-103, :184-185) ----
-    int *counter = reinterpret_cast<int *>(a.scratch + 4 * (size_t)M);
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(counter, 1) == nblocks - 1);
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    double esq = 0.0, esqc = 0.0, emax = 0.0;
-    bool bad = false;
-    for (int q = tid; q < nn; q += blockDim.x) {
-        const double ev = *((volatile double *)&a.E[a.n + q]);
-        const double v = a.xw[q % a.n] * (ev * ev);
-        const double t = esq + v;
-        esqc += (fabs(esq) >= fabs(v)) ? ((esq - t) + v) : ((v - t) + esq);
-        esq = t;
-        emax = fmax(emax, fabs(a.accel * ev));
-        bad |= !isfinite(ev);
-    }
-    const double energy = 0.5 * block_sum_dd(esq, esqc, s_red);
-    const double maxE = block_max(emax, s_max);
-    const int any_bad = __syncthreads_or(bad ? 1 : 0);
-    if (tid == 0) {
-        *counter = 0;
-        // get_max_speeds + adapt_time_step (main/timestep.py:231-242)
-        const double ab = a.accel * a.bfield;
-        const double s0 = fabs(a.umax);
-        const double s1 = fabs(maxE + fabs(ab * a.vmax));
-        const double s2 = fabs(a.accel * fabs(a.bfield * a.umax));
-        const double dtn = a.courant / (((s0 / a.dx) + (s1 / a.du)) + (s2 / a.dv));
-        const int64_t steps = st->steps + 1;
-        const double time = st->time + dtn;
-        st->dt_next = dtn;
-        st->time = time;
-        st->steps = steps;
-        const int cap = st->hist_capacity;
-        if (cap > 0) {
-            const int slot = (int)((steps - 1) % cap);
-            if (st->energy_hist) st->energy_hist[slot] = energy;
-            if (st->time_hist) st->time_hist[slot] = time;
-            if (st->dt_hist) st->dt_hist[slot] = dtn;
-        }
-        const bool finite = isfinite(energy) && isfinite(dtn) && !any_bad;
-        if (!finite) st->status |= 1;
-        st->active_next = (time < st->final_time) && (steps < st->max_steps) && finite;
-    }
-}
-
-static __global__ void __launch_bounds__(FIELD_THREADS) field_inv_kernel(const FieldArgs a) {
-    pdl_wait();
-    pdl_trigger();
-    field_inv_body(a, blockIdx.x, gridDim.x);
 }
 
 // energy + dt from a given E (vl_field_energy / vl_adapt_dt / vl_run_state_init)

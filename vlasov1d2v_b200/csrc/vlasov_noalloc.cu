@@ -1,6 +1,5 @@
-// SSP-RK3 loop entry point that allocates nothing: the loop's scratch (moment partials, field
-// mode coefficients, ticket counter) lives in a file-scope device array instead of a
-// caller-provided workspace.
+// SSP-RK3 loop entry point that allocates nothing: the loop's scratch (the moment partials of the
+// stage kernels) lives in a file-scope device array instead of a caller-provided workspace.
 //
 // Some callers cannot allocate device memory themselves: a host that records the loop into a
 // CUDA graph while allocations are forbidden, a plugin whose host framework owns the whole
@@ -11,17 +10,20 @@
 //   * capacity VL_NOALLOC_SCRATCH_BYTES (1 MiB) per GPU, held by every GPU that loads the
 //     library until the process exits;
 //   * its device address is looked up once per device with cudaGetSymbolAddress, on the first
-//     call made with that device current (make that first call outside any stream capture);
-//   * all calls share it and it keeps the last call's contents; the loop rewrites every entry
-//     it reads before reading it, and the one word that must start at zero (the field solve's
-//     ticket counter) is cleared by vl_ssp_rk3_steps on the call's stream; calls whose kernels
-//     overlap on the GPU (different streams, different contexts) race on it.
+//     call made with that device current (make that first call outside any stream capture); the
+//     cached address is not refreshed, so after a cudaDeviceReset the process must not call
+//     this entry point again on that device;
+//   * the call must be made with the context's own device current (checked);
+//   * all calls share it and it keeps the last call's contents; the loop writes every entry it
+//     reads before reading it (nothing has to start at zero); calls whose kernels overlap on
+//     the GPU (different streams, different contexts) race on it.
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <string>
 
 #include "vlasov1d2v.h"
+#include "vlasov_ctx.cuh"
 
 #define VL_NOALLOC_SCRATCH_DOUBLES (VL_NOALLOC_SCRATCH_BYTES / 8)
 
@@ -59,6 +61,14 @@ VL_API int vl_ssp_rk3_steps_noalloc(vl_ctx *ctx, void *f, void *stage_a, void *s
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
         vl_internal_set_error("vl_ssp_rk3_steps_noalloc: no usable current device");
         return VL_ERR_CUDA;
+    }
+    if (dev != ctx->device) {
+        // the scratch address is per device: the context's tables and the scratch must be on
+        // the same GPU
+        const std::string msg = "vl_ssp_rk3_steps_noalloc: current device " + std::to_string(dev) +
+                                " is not the context's device " + std::to_string(ctx->device);
+        vl_internal_set_error(msg.c_str());
+        return VL_ERR_INVALID;
     }
     void *scratch = nullptr;
     {

@@ -379,8 +379,6 @@ __device__ __forceinline__ void pencil_body_per_warp(const StageArgs &a, const T
 template <int N, typename T>
 __global__ void __launch_bounds__(PencilGeom<N, T>::THREADS, PencilGeom<N, T>::MIN_BLOCKS)
 stage_pencil_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
-    pdl_wait();
-    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
     pencil_body_per_warp<N, T, PencilGeom<N, T>::JC, PencilGeom<N, T>::THREADS, StageTables<T>>(
         a, tb, tb.qw, blockIdx.y, blockIdx.x, gridDim.x, (int)(threadIdx.x >> 5));

@@ -42,19 +42,9 @@
 #ifndef VL_FRAG_MINB32
 #define VL_FRAG_MINB32 4
 #endif
-// FP32 x / v contractions as error-compensated TF32 tensor-core products (0: FMA form)
-// (measured 4% slower than the FMA form on B200, and no more accurate: off by default)
-#ifndef VL_FRAG_TF32
-#define VL_FRAG_TF32 0
-#endif
 // warps per v element (each takes n / JS consecutive j rows)
 #ifndef VL_FRAG_JS64
 #define VL_FRAG_JS64 1
-#endif
-// stage buffers released per warp on an "empty" barrier that the issuing thread waits on (1),
-// or by a CTA-wide barrier after each tile (0)
-#ifndef VL_FRAG_EMPTYBAR
-#define VL_FRAG_EMPTYBAR 0
 #endif
 #ifndef VL_FRAG_JS32
 #define VL_FRAG_JS32 1
@@ -77,7 +67,6 @@ struct FragGeom {
     static constexpr int NJ = N / JS;                // j rows per warp
     static constexpr int THREADS = 32 * EPT * JS;
     static constexpr bool MMA = sizeof(T) == 8;      // tensor-core x/v contractions (FP64)
-    static constexpr bool TF32 = sizeof(T) == 4 && VL_FRAG_TF32;   // FP32: compensated TF32 products
     static constexpr int MINB = sizeof(T) == 8 ? VL_FRAG_MINB64 : VL_FRAG_MINB32;   // CTAs per SM
     static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
     static constexpr size_t IN_B = al(sizeof(T) * (size_t)PS * N);
@@ -113,35 +102,6 @@ __device__ __forceinline__ void dmma_8x8x4(double &d0, double &d1, double a, dou
         : "d"(a), "d"(b));
 }
 
-// FP32 operand as TF32 (round to nearest, ties away), and the error-compensated split
-// x = hi + lo with both parts TF32: a product of two split operands summed over hi*hi + hi*lo +
-// lo*hi (+ lo*lo) keeps close to FP32 accuracy on the TF32 tensor cores
-__device__ __forceinline__ uint32_t f2tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
-    hi = f2tf32(x);
-    lo = f2tf32(x - __uint_as_float(hi));
-}
-__device__ __forceinline__ void split_tf32(double x, uint32_t &hi, uint32_t &lo) {
-    hi = f2tf32((float)x);
-    lo = f2tf32((float)(x - (double)__uint_as_float(hi)));
-}
-
-// D[16x8] += A[16x8] B[8x8], TF32 operands, FP32 accumulation; per lane (g = lane/4, t = lane%4):
-// a = A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; b = B[t][g], B[t+4][g];
-// d = D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1]
-__device__ __forceinline__ void mma_tf32_16x8x8(float &d0, float &d1, float &d2, float &d3, uint32_t a0,
-                                                uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
-                                                uint32_t b1) {
-    asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};"
-        : "+f"(d0), "+f"(d1), "+f"(d2), "+f"(d3)
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
 template <typename T>
 struct Pair;
 template <>
@@ -161,17 +121,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     using V2 = typename Pair<T>::V;
     constexpr int N = G::N, P = G::P, W = G::W, PS = G::PS, WF = G::WF, PSF = G::PSF;
     constexpr int COLS = G::COLS, EPT = G::EPT, NT = G::THREADS;
-    // loop state written two or more launches back: readable before the dependency wait
-    if (a.state != nullptr && a.state->active == 0) {
-        pdl_wait();
-        return;
-    }
+    if (a.state != nullptr && a.state->active == 0) return;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     __shared__ __align__(8) uint64_t full[2];
-    __shared__ __align__(8) uint64_t empty[2];   // VL_FRAG_EMPTYBAR: one arrival per warp and tile
     __shared__ dd sRed[EPT * G::JS][N];
 
     const int tid = threadIdx.x;
@@ -209,8 +164,6 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     if (tid == 0) {
         mbar_init(&full[0], 1);
         mbar_init(&full[1], 1);
-        mbar_init(&empty[0], NT / 32);
-        mbar_init(&empty[1], NT / 32);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -244,10 +197,6 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         if (ntile_cta > 0) issue(0, 0);
         if (ntile_cta > 1) issue(1, 1);
     }
-    // the first tiles (the previous stage's output) stream in while the field solve finishes;
-    // E comes from the immediately preceding launch
-    pdl_wait();
-    pdl_trigger();
 
     const double accel = a.accel, bfield = a.bfield;
     const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
@@ -260,13 +209,9 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     // only the neighbour trace remains as a lift: xi[g][0] (x, from the left) / -xi[g][1] (x, from
     // the right) for the x direction, xi[k][0] / -xi[k][1] of the thread's columns k for v
     T ca0, ca1, ca0M, ca1P, xil, xir, vil0, vil1, vir0, vir1;
-    // TF32 form: the same folded fragments (P: speed >= 0, M: speed < 0) split hi + lo from the
-    // FP64 tables; they serve as the x product's A rows (hi rows 0-7, lo rows 8-15) and as the
-    // v product's B operand
-    uint32_t uP0h, uP0l, uP1h, uP1l, uM0h, uM0l, uM1h, uM1l;
     T upi[N], upk0[N], upk1[N];    // FMA form: up[g][.], up[2t][.], up[2t + 1][.]
     T xig0, xig1, xik00, xik01, xik10, xik11;
-    if constexpr (G::MMA || G::TF32) {
+    if constexpr (G::MMA) {
         xil = tb.xi[2 * g];
         xir = -tb.xi[2 * g + 1];
         vil0 = tb.xi[4 * t];
@@ -274,14 +219,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         vir0 = -tb.xi[4 * t + 1];
         vir1 = -tb.xi[4 * t + 3];
     }
-    if constexpr (G::TF32) {
-        const double *dup = a.tables;            // up [n n] in FP64
-        const double *dxi = a.tables + N * N;    // xi [n 2]
-        split_tf32(dup[g * N + t], uP0h, uP0l);
-        split_tf32(t == 3 ? dup[g * N + 7] - dxi[2 * g + 1] : dup[g * N + 4 + t], uP1h, uP1l);
-        split_tf32(t == 0 ? dup[g * N] + dxi[2 * g] : dup[g * N + t], uM0h, uM0l);
-        split_tf32(dup[g * N + 4 + t], uM1h, uM1l);
-    } else if constexpr (G::MMA) {
+    if constexpr (G::MMA) {
         ca0 = tb.up[g * N + t];
         ca1 = tb.up[g * N + 4 + t];
         ca0M = tb.upM[g * N + t];
@@ -381,34 +319,6 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                         const T vn = vpos ? pa[-1] : pa[N];
                         dv0 = fma(vpos ? vil0 : vir0, vn, v0);
                         dv1 = fma(vpos ? vil1 : vir1, vn, v1);
-                    } else if constexpr (G::TF32) {
-                        // x: [U_hi; U_lo] (rows g, g + 8) times F_j, hi then lo parts
-                        const T *pb = sIn + j * W + P + wc + g;
-                        uint32_t bh0, bl0, bh1, bl1;
-                        split_tf32((float)pb[t * PS], bh0, bl0);
-                        split_tf32((float)pb[(4 + t) * PS], bh1, bl1);
-                        const uint32_t x0h = xpos ? uP0h : uM0h, x0l = xpos ? uP0l : uM0l;
-                        const uint32_t x1h = xpos ? uP1h : uM1h, x1l = xpos ? uP1l : uM1l;
-                        float d0 = 0.f, d1 = 0.f, d2 = 0.f, d3 = 0.f;
-                        mma_tf32_16x8x8(d0, d1, d2, d3, x0h, x0l, x1h, x1l, bh0, bh1);
-                        mma_tf32_16x8x8(d0, d1, d2, d3, x0h, x0l, x1h, x1l, bl0, bl1);
-                        const V2 xn = *reinterpret_cast<const V2 *>(sXF + (xpos ? 0 : N * COLS) + j * COLS + cl);
-                        const T xcn = xpos ? xil : xir;
-                        dx0 = fma(xcn, xn.x, (T)(d0 + d2));
-                        dx1 = fma(xcn, xn.y, (T)(d1 + d3));
-                        // v: [F_hi; F_lo] (rows g, g + 8; k index m) times U^T, hi then lo parts
-                        const T *pa = prow + j * W;
-                        uint32_t ah0, al0, ah1, al1;
-                        split_tf32((float)pa[t], ah0, al0);
-                        split_tf32((float)pa[4 + t], ah1, al1);
-                        const uint32_t v0h = vpos ? uP0h : uM0h, v0l = vpos ? uP0l : uM0l;
-                        const uint32_t v1h = vpos ? uP1h : uM1h, v1l = vpos ? uP1l : uM1l;
-                        float e0 = 0.f, e1 = 0.f, e2 = 0.f, e3 = 0.f;
-                        mma_tf32_16x8x8(e0, e1, e2, e3, ah0, al0, ah1, al1, v0h, v1h);
-                        mma_tf32_16x8x8(e0, e1, e2, e3, ah0, al0, ah1, al1, v0l, v1l);
-                        const T vn = vpos ? pa[-1] : pa[N];
-                        dv0 = fma(vpos ? vil0 : vir0, vn, (T)(e0 + e2));
-                        dv1 = fma(vpos ? vil1 : vir1, vn, (T)(e1 + e3));
                     } else {
                         const T *pc = sIn + j * W + P + cl;   // F[m][j][cl..cl+1] at m = 0
                         dx0 = (T)0;
@@ -500,26 +410,9 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     rows(std::integral_constant<int, G::NJ>{});
             }
         }
-#if VL_FRAG_EMPTYBAR
-        // this warp is done with stage s; the issuing thread waits for every warp (use q >> 1 of
-        // the barrier) before refilling it, the other warps go on to the next tile
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-        if (tid == 0 && q + 2 < ntile_cta) {
-            if (!mbar_wait_bounded(&empty[s], (uint32_t)((q >> 1) & 1))) {
-                if (a.err != nullptr) atomicOr(a.err, 2);
-                return;
-            }
-            issue(s, q + 2);
-        }
-#else
         __syncthreads();   // stage s fully consumed
         if (tid == 0 && q + 2 < ntile_cta) issue(s, q + 2);
-#endif
     }
-#if VL_FRAG_EMPTYBAR
-    __syncthreads();   // every warp is out of the tile loop before the shared reduction
-#endif
 
     if (a.partials == nullptr) return;
     // moment partial of x node g: sum over the thread's columns, the quad, the warps

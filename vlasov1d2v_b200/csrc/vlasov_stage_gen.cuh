@@ -35,14 +35,6 @@
 // (off < 16 bytes per tile), and the column pairs are read as two scalar loads.  Every box lands
 // on a 128-byte-aligned shared-memory address.
 //
-// Phased form (FP32 rows that are not 16-byte multiples): every thread copies 16-byte chunks
-// with cp.async into contiguous rows, each row starting at the 16-byte boundary at or below the
-// tile's left v trace.  The offset of that trace inside the row ("phase", 0-3 floats) depends on
-// the row's position in the state; when (nu+2) n (nv+2) n is a multiple of 4 all rows of one j
-// (input, f^n, x faces, background) share one phase, (K0 + j (nv+2) n) mod 4 with K0 fixed per
-// tile, and the two u-face rows have their own.  The compute adds that per-j offset to its
-// columns and reads the pairs as two scalar loads.  Row lengths hold an odd number of 16-byte units and planes an odd number of rows, so
-// the loads of eight x nodes at one column fall in distinct banks.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -217,37 +209,8 @@ struct GenTmaGeom {
     static_assert(WB <= 256, "TMA box width");
 };
 
-template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
-struct GenPhGeom {
-    static_assert(sizeof(T) == 4, "the phased form serves FP32 states");
-    static constexpr int EPT = EPT_;
-    static constexpr int WC = EPT * N + 2;                       // columns needed: tile + both traces
-    static constexpr int RS0 = (WC + 3 + 3) / 4 * 4;             // row slot: any phase, 16-byte units
-    static constexpr int RS = ((N * RS0 / 4) % 2 == 1) ? RS0 : RS0 + 4;   // odd 16-byte units per plane
-    static constexpr int PS = N * RS;
-    static constexpr int THREADS = GenGeom<N, T, EPT>::THREADS;
-    static constexpr int NST = 2;
-    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
-    static constexpr size_t IN_B = al(sizeof(T) * (size_t)N * PS);
-    static constexpr size_t FN_B = IN_B;
-    static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * N * RS);
-    static constexpr size_t UF_B = XF_B;
-    static constexpr size_t BG_B = al(sizeof(float) * (size_t)2 * N * RS);
-    static constexpr size_t UX_B = al(sizeof(double) * (size_t)N);
-    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
-    static constexpr size_t smem_bytes() {
-        const size_t s = NST * STAGE_B;
-        const size_t red = sizeof(dd) * (size_t)THREADS;
-        return (s > red ? s : red) + 128;
-    }
-    static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
-    static constexpr int REG_CTAS = 65536 / ((THREADS + 63) / 64 * 64 * 128);
-    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
-    static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
-};
-
 // shared-memory layout constants of the three forms (row lengths, plane strides, array bytes):
-// MODE 0 slot rows (cp.async), 1 TMA rows, 2 phased rows (cp.async)
+// MODE 0 slot rows (cp.async), 1 TMA rows
 template <int MODE, int N, typename T, int EPT>
 struct GenLayout {
     using GG = GenGeom<N, T, EPT>;
@@ -256,15 +219,6 @@ struct GenLayout {
     static constexpr int BGS = N * GG::WF;  // offset of the second background table (floats)
     static constexpr size_t S_IN = GG::IN_B, S_FN = GG::FN_B, S_XF = GG::XF_B, S_UF = GG::UF_B;
     static constexpr size_t S_BG = GG::BG_B, S_STAGE = GG::STAGE_B;
-};
-template <int N, typename T, int EPT>
-struct GenLayout<2, N, T, EPT> {
-    using GP = GenPhGeom<N, T, EPT>;
-    static constexpr int RIN = GP::RS, PIN = GP::PS, RFN = GP::RS, PFN = GP::PS, RFC = GP::RS, Q = 4;
-    static constexpr int FS = N * GP::RS;
-    static constexpr int BGS = N * GP::RS;
-    static constexpr size_t S_IN = GP::IN_B, S_FN = GP::FN_B, S_XF = GP::XF_B, S_UF = GP::UF_B;
-    static constexpr size_t S_BG = GP::BG_B, S_STAGE = GP::STAGE_B;
 };
 template <int N, typename T, int EPT>
 struct GenLayout<1, N, T, EPT> {
@@ -291,19 +245,18 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PH = false, bool BULK = false>
+template <int N, typename T, int EPT, typename TB, bool TMA = false>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
                                                int g, int G, unsigned char *smem,
                                                const GenMaps *maps = nullptr) {
-    static_assert(!BULK || PH, "bulk copies fill the phased rows");
-    constexpr bool CONTIG = TMA || PH;   // contiguous rows (scalar pair loads)
-    constexpr bool MB = TMA || BULK;     // stages filled by asynchronous bulk copies on mbarriers
+    constexpr bool CONTIG = TMA;   // contiguous rows (scalar pair loads)
+    constexpr bool MB = TMA;       // stages filled by asynchronous bulk copies on mbarriers
     using GG = GenGeom<N, T, EPT>;
     using V2 = typename GenPair<T>::V;
     constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
     constexpr int PS = GG::PS, PSF = GG::PSF, NST = GG::NST, NW = GG::NW, NT = GG::THREADS;
     // shared-memory geometry of the form in use (TMA: contiguous rows of the state)
-    using L = GenLayout<TMA ? 1 : (PH ? 2 : 0), N, T, EPT>;
+    using L = GenLayout<TMA ? 1 : 0, N, T, EPT>;
     constexpr int RIN = L::RIN;      // IN row length
     constexpr int PIN = L::PIN;      // IN plane stride
     constexpr int RFN = L::RFN;      // FN row length
@@ -439,145 +392,6 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         }
         if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
     };
-    // phased form: 16-byte chunks of each row from the 16-byte boundary at or below the tile's
-    // left v trace through its right v trace (at most 3 floats more, still inside the array: the
-    // row after the last one read always exists); a warp per row.  VN = (nv + 2) n floats per row, base pointers 16-byte aligned.
-    auto issue_ph = [&](int s, int tt) {
-        if constexpr (PH) {
-            using GP = GenPhGeom<N, T, EPT>;
-            const int au = tt / nbt;
-            const int b0 = (tt - au * nbt) * EPT;
-            const int nb = min(EPT, nv - b0);
-            const int Ag = au + 1;
-            const size_t cg0 = (size_t)(b0 + 1) * N - 1;
-            const int wc = nb * N + 2;   // the tile's elements and both v traces (<= GP::WC)
-            unsigned char *st = stage_ptr(s);
-            T *dIn = reinterpret_cast<T *>(st);
-            T *dFn = reinterpret_cast<T *>(st + S_IN);
-            T *dXF = reinterpret_cast<T *>(st + S_IN + S_FN);
-            T *dUF = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF);
-            float *dBG = reinterpret_cast<float *>(st + S_IN + S_FN + S_XF + S_UF);
-            double *dUX = reinterpret_cast<double *>(st + S_IN + S_FN + S_XF + S_UF + S_BG);
-            // row r of a [rows][VN] array starting at base: the needed run from column cg0
-            auto row = [&](T *dst, const T *base, size_t r) {
-                const size_t A0 = r * (size_t)sJ + cg0;
-                const size_t S0 = A0 & ~(size_t)3;
-                const int nch = (int)((A0 - S0 + wc + 3) >> 2);
-                for (int k = lane; k < nch; k += 32) cp_async<16>(dst + 4 * k, base + S0 + 4 * k);
-            };
-            // row index of (e, i, a, j) in the state
-            auto sr = [&](int ee, int ii, int aa, int jj) -> size_t {
-                return (((size_t)ee * N + ii) * U + aa) * N + jj;
-            };
-            for (int r = warp; r < N * N; r += NW) {
-                const int ii = r / N, jj = r - ii * N;
-                row(dIn + ii * GP::PS + jj * GP::RS, in, sr(Eg, ii, Ag, jj));
-                if (with_fn) row(dFn + ii * GP::PS + jj * GP::RS, fn, sr(Eg, ii, Ag, jj));
-            }
-            for (int r = warp; r < 4 * N; r += NW) {
-                const int side = (r / N) & 1, q = r % N;
-                if (r < 2 * N)   // x traces: row j = q of (El, i = n-1) / (Er, i = 0)
-                    row(dXF + (side * N + q) * GP::RS, in, sr(side ? Er : El, side ? 0 : N - 1, Ag, q));
-                else             // u traces: row i = q of (a-1, j = n-1) / (a+1, j = 0)
-                    row(dUF + (side * N + q) * GP::RS, in, sr(Eg, q, side ? Ag + 1 : Ag - 1, side ? 0 : N - 1));
-            }
-            if (with_bg) {
-                for (int r = warp; r < 2 * N; r += NW) {
-                    const int tbl = r / N, jj = r % N;
-                    row(dBG + (tbl * N + jj) * GP::RS, tbl ? a.bg_rb : a.bg_eu, (size_t)Ag * N + jj);
-                }
-            }
-            if (tid < N) cp_async<8>(dUX + tid, a.u_nodes + Ag * N + tid);
-        } else {
-            (void)s;
-            (void)tt;
-        }
-    };
-    // phased rows by bulk copies (warp 0): the same row runs as the phased form, each one
-    // cp.async.bulk from its 16-byte boundary (16-byte multiples), completing on gfull[s] with
-    // the exact byte total announced first; the u nodes from the even index at or below Ag n
-    auto issue_phb = [&](int s, int tt) {
-        if constexpr (BULK) {
-            using GP = GenPhGeom<N, T, EPT>;
-            const int au = tt / nbt;
-            const int b0 = (tt - au * nbt) * EPT;
-            const int nb = min(EPT, nv - b0);
-            const int Ag = au + 1;
-            const size_t cg0 = (size_t)(b0 + 1) * N - 1;
-            const int wc = nb * N + 2;   // the tile's elements and both v traces (<= GP::WC)
-            unsigned char *st = stage_ptr(s);
-            T *dIn = reinterpret_cast<T *>(st);
-            T *dFn = reinterpret_cast<T *>(st + S_IN);
-            T *dXF = reinterpret_cast<T *>(st + S_IN + S_FN);
-            T *dUF = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF);
-            T *dBG = reinterpret_cast<T *>(st + S_IN + S_FN + S_XF + S_UF);
-            double *dUX = reinterpret_cast<double *>(st + S_IN + S_FN + S_XF + S_UF + S_BG);
-            auto sr = [&](int ee, int ii, int aa, int jj) -> size_t {
-                return (((size_t)ee * N + ii) * U + aa) * N + jj;
-            };
-            const int n_in = N * N, n_fn = with_fn ? N * N : 0, n_bg = with_bg ? 2 * N : 0;
-            const int nrow = n_in + n_fn + 4 * N + n_bg;
-            // row q of the tile: its shared destination, source array and row index
-            auto row_of = [&](int q, T *&dst, const T *&src, size_t &r) {
-                if (q < n_in + n_fn) {
-                    const int qq = q < n_in ? q : q - n_in;
-                    const int ii = qq / N, jj = qq - (qq / N) * N;
-                    dst = (q < n_in ? dIn : dFn) + ii * GP::PS + jj * GP::RS;
-                    src = q < n_in ? in : fn;
-                    r = sr(Eg, ii, Ag, jj);
-                    return;
-                }
-                q -= n_in + n_fn;
-                if (q < 4 * N) {
-                    const int side = (q / N) & 1, qq = q % N;
-                    src = in;
-                    if (q < 2 * N) {   // x traces: row j = qq of (El, i = n-1) / (Er, i = 0)
-                        dst = dXF + (side * N + qq) * GP::RS;
-                        r = sr(side ? Er : El, side ? 0 : N - 1, Ag, qq);
-                    } else {           // u traces: row i = qq of (a-1, j = n-1) / (a+1, j = 0)
-                        dst = dUF + (side * N + qq) * GP::RS;
-                        r = sr(Eg, qq, side ? Ag + 1 : Ag - 1, side ? 0 : N - 1);
-                    }
-                    return;
-                }
-                q -= 4 * N;
-                const int tbl = q / N, jj = q % N;   // background-split tables [U n][V n]
-                dst = dBG + (tbl * N + jj) * GP::RS;
-                src = reinterpret_cast<const T *>(tbl ? a.bg_rb : a.bg_eu);
-                r = (size_t)Ag * N + jj;
-            };
-            auto span = [&](size_t r, size_t &s0) -> uint32_t {
-                const size_t a0 = r * (size_t)sJ + cg0;
-                s0 = a0 & ~(size_t)3;
-                return (uint32_t)(((a0 - s0 + wc + 3) >> 2) * 16);
-            };
-            const uint32_t ux_bytes = (uint32_t)sizeof(double) * (N + (N & 1));
-            uint32_t total = 0;
-            for (int q = lane; q < nrow; q += 32) {
-                T *dst;
-                const T *src;
-                size_t r, s0;
-                row_of(q, dst, src, r);
-                total += span(r, s0);
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) total += __shfl_xor_sync(0xffffffffu, total, off);
-            if (lane == 0) mbar_arrive_expect_tx(&gfull[s], total + ux_bytes);
-            __syncwarp();
-            for (int q = lane; q < nrow; q += 32) {
-                T *dst;
-                const T *src;
-                size_t r, s0;
-                row_of(q, dst, src, r);
-                const uint32_t bytes = span(r, s0);
-                bulk_load(dst, src + s0, bytes, &gfull[s]);
-            }
-            if (lane == 0) bulk_load(dUX, a.u_nodes + ((Ag * N) & ~1), ux_bytes, &gfull[s]);
-        } else {
-            (void)s;
-            (void)tt;
-        }
-    };
     // TMA form: one thread loads the tile's boxes into stage s
     auto issue_tma = [&](int s, int tt) {
         if constexpr (TMA) {
@@ -632,32 +446,17 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             if (ntile > 0) issue_tma(0, g);
             if (ntile > 1) issue_tma(1, g + G);
         }
-    } else if constexpr (BULK) {
-        if (warp == 0) {
-            if (ntile > 0) issue_phb(0, g);
-            if (ntile > 1) issue_phb(1, g + G);
-        }
     } else {
 #pragma unroll
         for (int s0 = 0; s0 < NST - 1; ++s0) {
-            if (s0 < ntile) {
-                if constexpr (PH)
-                    issue_ph(s0, g + s0 * G);
-                else
-                    issue(s0, g + s0 * G);
-            }
+            if (s0 < ntile) issue(s0, g + s0 * G);
             cp_async_commit();
         }
     }
     for (int q = 0; q < ntile; ++q) {
         if constexpr (!MB) {
             const int qn = q + NST - 1;
-            if (qn < ntile) {
-                if constexpr (PH)
-                    issue_ph(qn % NST, g + qn * G);
-                else
-                    issue(qn % NST, g + qn * G);
-            }
+            if (qn < ntile) issue(qn % NST, g + qn * G);
             cp_async_commit();
         }
         const int tt = g + q * G;
@@ -687,21 +486,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         // column of element b's node 0 in the IN rows, of the thread's pair in IN and in the
         // FN / face / background rows; first u node in sUX
         const int cL = (b0 + 1) * N - 1;
-        const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : (PH ? 1 + b * N : H + b * SL);
+        const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : H + b * SL;
         const int cin = ebase + 2 * p;
         const int cfc = CONTIG ? cin : cs;
-        // phased form: offset of the rows of index j (input, f^n, x faces, background) and of
-        // the two u-face rows inside their slots
-        const int K0 = (int)(((unsigned)Ag * (unsigned)N * (unsigned)sJ + (unsigned)cL) & 3u);
-        const int KJ = sJ & 3;
-        auto jsh = [&](int jj) -> int {
-            if constexpr (PH)
-                return (K0 + jj * KJ) & 3;
-            else
-                return 0;
-        };
-        const int ush0 = PH ? ((K0 - KJ) & 3) : 0;
-        const int ush1 = PH ? ((K0 + N * KJ) & 3) : 0;
         const double *sUX = sUX0 + (MB ? ((Ag * N) & 1) : 0);
         auto ld2 = [&](const T *q2) -> V2 {
             if constexpr (CONTIG) {
@@ -719,9 +506,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             const T sp0 = (T)sd0, sp1 = (T)sd1;
             V2 fu[N];
 #pragma unroll
-            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin + jsh(m));
-            const V2 ufl = ld2(sUF + i * RFC + cfc + ush0);
-            const V2 ufr = ld2(sUF + FS + i * RFC + cfc + ush1);
+            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin);
+            const V2 ufl = ld2(sUF + i * RFC + cfc);
+            const V2 ufr = ld2(sUF + FS + i * RFC + cfc);
             const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
             const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
             T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
@@ -733,7 +520,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 const bool xpos = uxd >= 0.0;
                 const bool vpos = svd >= 0.0;
                 // x: sum_m up[i][m] F[m][j][k] + lifts
-                const T *pc = sIn + j * RIN + cin + jsh(j);
+                const T *pc = sIn + j * RIN + cin;
                 T dx0 = (T)0, dx1 = (T)0;
                 V2 cm0, cmL;
 #pragma unroll
@@ -744,8 +531,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     dx0 = fma(upi[m], cv.x, dx0);
                     dx1 = fma(upi[m], cv.y, dx1);
                 }
-                const V2 xf0 = ld2(sXF + j * RFC + cfc + jsh(j));
-                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc + jsh(j));
+                const V2 xf0 = ld2(sXF + j * RFC + cfc);
+                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc);
                 const V2 xl = xpos ? xf0 : cm0;
                 const V2 xr = xpos ? cmL : xf1;
                 dx0 = fma(xig0, xl.x, dx0);
@@ -753,7 +540,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 dx1 = fma(xig0, xl.y, dx1);
                 dx1 = fma(-xig1, xr.y, dx1);
                 // v: sum_m F[i][j][m] up[k][m] + lifts (the element's k-line)
-                const T *pa = prow + j * RIN + jsh(j);
+                const T *pa = prow + j * RIN;
                 T line[2 * P];
 #pragma unroll
                 for (int m2 = 0; m2 < P; ++m2) {
@@ -789,7 +576,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
                 if (with_bg) {   // RHS of the x-independent background
                     float2 eu, rb;
-                    const float *pbg = sBG + j * RFC + cfc + jsh(j);
+                    const float *pbg = sBG + j * RFC + cfc;
                     if constexpr (CONTIG) {
                         eu = make_float2(pbg[0], pbg[1]);
                         rb = make_float2(pbg[L::BGS], pbg[L::BGS + 1]);
@@ -809,7 +596,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     o.x = fma(dtT, r0, fij.x);
                     o.y = fma(dtT, r1, fij.y);
                 } else {
-                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc + jsh(j));
+                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc);
                     o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
                     o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
                 }
@@ -839,8 +626,6 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         __syncthreads();   // stage q % NST consumed before it is refilled
         if constexpr (TMA) {
             if (tid == 0 && q + 2 < ntile) issue_tma(q & 1, g + (q + 2) * G);
-        } else if constexpr (BULK) {
-            if (warp == 0 && q + 2 < ntile) issue_phb(q & 1, g + (q + 2) * G);
         }
     }
     cp_async_wait<0>();
@@ -863,8 +648,6 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
 template <int N, typename T>
 __global__ void __launch_bounds__(GenGeom<N, T>::THREADS, GenGeom<N, T>::MINB)
 stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
-    pdl_wait();
-    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
@@ -872,41 +655,11 @@ stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
     gen_stage_body<N, T, GenGeom<N, T>::EPT>(a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
-// phased form (FP32 rows that are not 16-byte multiples)
-template <int N>
-__global__ void __launch_bounds__(GenPhGeom<N, float>::THREADS, GenPhGeom<N, float>::MINB)
-stage_gen_ph_kernel(const StageArgs a, const __grid_constant__ StageTables<float> tb) {
-    pdl_wait();
-    pdl_trigger();
-    if (a.state != nullptr && a.state->active == 0) return;
-    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
-    unsigned char *base = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
-    gen_stage_body<N, float, GenGeom<N, float>::EPT, StageTables<float>, false, true>(
-        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
-}
-
-// phased rows filled by bulk copies on mbarriers (FP32, any row alignment)
-template <int N>
-__global__ void __launch_bounds__(GenPhGeom<N, float>::THREADS, GenPhGeom<N, float>::MINB)
-stage_gen_phb_kernel(const StageArgs a, const __grid_constant__ StageTables<float> tb) {
-    pdl_wait();
-    pdl_trigger();
-    if (a.state != nullptr && a.state->active == 0) return;
-    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
-    unsigned char *base = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
-    gen_stage_body<N, float, GenGeom<N, float>::EPT, StageTables<float>, false, true, true>(
-        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
-}
-
 // TMA form (16-byte-aligned state rows)
 template <int N, typename T>
 __global__ void __launch_bounds__(GenTmaGeom<N, T>::THREADS, GenTmaGeom<N, T>::MINB)
 stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                      const __grid_constant__ GenMaps maps) {
-    pdl_wait();
-    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(

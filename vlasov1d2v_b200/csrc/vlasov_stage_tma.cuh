@@ -174,8 +174,6 @@ stage_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     using G = TmaGeom<N, T>;
     constexpr int P = G::P, EPW = G::EPW, COLS = G::COLS, W = G::W, JC = G::JC, NT = G::THREADS;
     constexpr int VEC = G::VEC;
-    pdl_wait();
-    pdl_trigger();
     if (a.state != nullptr && a.state->active == 0) return;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -27,37 +27,11 @@ class Elliptic:
 
     # -- DG central-flux operator (main/elliptic.py:24-83), host set-up ----------------------------
     def build_central_flux_operator(self, grid, basis):
-        res, order = grid.res, grid.order
-        indicator = np.zeros((res, order))
-        face_diff0 = np.zeros((res, 2))
-        face_diff1 = np.zeros((res, 2))
-        num_flux = np.zeros_like(face_diff0)
-        grad_num_flux = np.zeros_like(face_diff1)
-        op = np.zeros((res, order, res, order))
-        grad_op = np.zeros_like(op)
-        for i in range(res):
-            for j in range(order):
-                indicator[i, j] = 1.0
-                face_diff0[:, 0] = indicator[:, 0] - np.roll(indicator[:, -1], 1)
-                face_diff0[:, 1] = indicator[:, -1] - np.roll(indicator[:, 0], -1)
-                num_flux[:, 0] = 0.5 * face_diff0[:, 0]
-                num_flux[:, 1] = -0.5 * face_diff0[:, 1]
-                grad = (np.tensordot(basis.der, indicator, axes=([1], [1])) +
-                        np.tensordot(basis.np_xi, num_flux, axes=([1], [1]))).T
-                face_diff1[:, 0] = grad[:, 0] - np.roll(grad[:, -1], 1)
-                face_diff1[:, 1] = grad[:, -1] - np.roll(grad[:, 0], -1)
-                grad_num_flux[:, 0] = 0.5 * face_diff1[:, 0]
-                grad_num_flux[:, 1] = -0.5 * face_diff1[:, 1]
-                operator = (np.tensordot(basis.stf, grad, axes=([1], [1])) +
-                            np.tensordot(basis.face_mass, grad_num_flux + face_diff0, axes=([1], [1]))).T
-                op[i, j, :, :] = operator
-                grad_op[i, j, :, :] = grad
-                indicator[i, j] = 0
-        qw = grid.np_quad_weights
-        op0 = np.hstack([op.reshape(res * order, res * order), qw.reshape(res * order, 1)])
-        self.central_flux_operator = np.vstack([op0, np.append(qw.flatten(), 0)])
-        self.central_flux_operator[np.abs(self.central_flux_operator) < 1.0e-15] = 0
-        self.gradient_operator = _device.wrap(torch.as_tensor(grad_op, device=_device.device()))
+        """The bordered central-flux Laplacian (host) and the DG gradient map (device) of
+        ``central_flux_matrices``."""
+        bordered, grad_src = central_flux_matrices(grid, basis)
+        self.central_flux_operator = bordered
+        self.gradient_operator = _device.wrap(torch.as_tensor(grad_src, device=_device.device()))
 
     def invert(self):
         self.inv_op = _device.wrap(torch.as_tensor(np.linalg.inv(self.central_flux_operator),
@@ -110,3 +84,40 @@ class Elliptic:
         out = torch.empty(1, dtype=torch.float64, device=E.device)
         ctx.field_energy(E, out)
         return _device.wrap(out[0])
+
+
+def central_flux_matrices(grid, basis):
+    """Bordered matrix of the DG central-flux Laplacian and the DG gradient map, host FP64.
+
+    Both are assembled directly as linear maps on the nodal vector q (length res n, element
+    major): with J0 q = q[e, 0] - q[e-1, n-1] and J1 q = q[e, n-1] - q[e+1, 0] the trace jumps at
+    the left and right face of every element (periodic), the gradient is
+    g = (I kron der) q + xi_L (J0 q) / 2 - xi_R (J1 q) / 2, and the operator is
+    (I kron stf) g + e_0 (J0 g / 2 + J0 q) + e_{n-1} (-J1 g / 2 + J1 q)
+    (face_mass selects the first and last node of each element).  The reference stores each map
+    with the source node first (row = source, column = destination), so both are returned in
+    that convention: the Laplacian bordered by the quadrature weights (zero-mean gauge row and
+    column) with entries below 1e-15 cleared, as ``main/elliptic.py:73-78`` does, and the
+    gradient as [i, j, e, k] = node (e, k) of the gradient of the unit vector at (i, j)."""
+    res, n = grid.res, grid.order
+    N = res * n
+    eye = np.eye(res)
+    nxt = np.roll(eye, 1, axis=1)    # (nxt x)[e] = x[e+1]
+    prv = np.roll(eye, -1, axis=1)   # (prv x)[e] = x[e-1]
+    first = np.kron(eye, np.eye(n)[:1])   # res x N: q[e, 0]
+    last = np.kron(eye, np.eye(n)[-1:])   # res x N: q[e, n-1]
+    jump_left = first - prv @ last
+    jump_right = last - nxt @ first
+    xi = basis.np_xi
+    lift_left = np.kron(eye, xi[:, :1])   # N x res: xi[:, 0] into element e
+    lift_right = np.kron(eye, xi[:, 1:])
+    grad = np.kron(eye, basis.der) + 0.5 * (lift_left @ jump_left) - 0.5 * (lift_right @ jump_right)
+    lap = (np.kron(eye, basis.stf) @ grad + first.T @ (0.5 * (jump_left @ grad) + jump_left) +
+           last.T @ (-0.5 * (jump_right @ grad) + jump_right))
+    qw = np.asarray(grid.np_quad_weights, dtype=np.float64).reshape(N)
+    bordered = np.zeros((N + 1, N + 1))
+    bordered[:N, :N] = lap.T
+    bordered[:N, N] = qw
+    bordered[N, :N] = qw
+    bordered[np.abs(bordered) < 1.0e-15] = 0
+    return bordered, np.ascontiguousarray(grad.T.reshape(res, n, res, n))

@@ -52,6 +52,13 @@ class Grid1D:
             self.np_grid_phases = np.exp(1j * np.tensordot(self.wave_numbers, self.arr[1:-1, :], axes=0))
             self.np_spectral_transform = basis.fourier_transform_array(self.midpoints, self.J,
                                                                        self.wave_numbers)
+            # the factors the native field solve uses: T[e, j, m] = phase[e, m] ell[j, m] and
+            # exp(i k_m x_{e,j}) = conj(phase[e, m]) qnode[j, m]
+            ell, phase = basis.fourier_factors(self.midpoints, self.J, self.wave_numbers)
+            self.np_dft_ell = np.ascontiguousarray(ell)
+            self.np_dft_phase = np.ascontiguousarray(phase)
+            self.np_dft_qnode = np.ascontiguousarray(
+                np.exp(1j * np.multiply.outer(self.arr[1] - self.midpoints[0], self.wave_numbers)))
         self._vl_cache = {}
 
     def create_grid(self, nodes):
