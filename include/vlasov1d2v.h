@@ -319,12 +319,17 @@ VL_API int vl_closure_features(const void *f, int32_t prec, int32_t nx, int32_t 
                                const double *E, double accel, double bfield, const double *u_nodes,
                                const double *v_nodes, double umax, double vmax, double escale, float *X,
                                float *scale, void *stream);
-/* out[e, i, a, j, b, k] += c2 * (*dt) * cscale * scale[s] * clamp(Y[s][6 j + k], +-ymax) for
- * every interior node: the network's RHS correction applied to an RK stage output, its outputs
- * clamped to the range seen in training (state may be NULL; an inactive loop state skips it).  */
+/* out[e, i, a, j, b, k] += c2 * (*dt) * cscale * c[s, j, k], c = scale[s] * clamp(Y[s][6 j + k],
+ * +-ymax), for every interior node: the network's RHS correction applied to an RK stage output,
+ * its outputs clamped to the range seen in training (state may be NULL; an inactive loop state
+ * skips it).  mode VL_CLOSURE_CHARGE subtracts from c, per x node, its quadrature mean over all
+ * velocity nodes (weights node_weights[j] node_weights[k], the 6 LGL weights; host pointer), so
+ * the correction conserves the charge density the field is solved from.                        */
+enum vl_closure_mode { VL_CLOSURE_PLAIN = 0, VL_CLOSURE_CHARGE = 1 };
 VL_API int vl_closure_apply(void *out, int32_t prec, int32_t nx, int32_t nu, int32_t nv, const float *Y,
                             const float *scale, double cscale, float ymax, const double *dt, double c2,
-                            const vl_run_state *state, void *stream);
+                            const vl_run_state *state, int32_t mode, const double *node_weights,
+                            void *stream);
 
 /* ---- the loop without a caller-provided workspace ------------------------------------------- */
 

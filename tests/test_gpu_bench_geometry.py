@@ -101,3 +101,37 @@ def test_fp32_background_split_steps_on_benchmark_velocity_grids(cuda, res, n):
     f = p.f.full_array().get()
     assert rel_err(f[INNER], f_ref[INNER]) < 2e-6
     assert history_err(p.stepper.field_energy, rec.field_energy) < 1e-5
+
+
+@pytest.mark.parametrize("res", [(2, 3, 5), (2, 50, 50)], ids=["ragged", "medium_slab"])
+def test_fp32_n8_directional_rhs_against_oracle(cuda, res):
+    """vl_rhs_weighted on the FP32 n = 8 kernel: the three single-direction RHS (x, u, v flux
+    terms, each with its Jacobian as the weight and the other two weights zero) sum to the
+    oracle's full RHS within FP32 rounding, and each of them is a non-trivial part of it."""
+    from vlasov1d2v_b200 import _lib, problem
+    from vlasov1d2v_b200.context import get_context
+
+    n = 8
+    p = problem.build(res, n, perturbation=None, amp=0.0, precision="fp32", background_split=False)
+    c = vo.make_case(*res, n)
+    ctx = get_context(p.grids, precision="fp32", accel=p.refs.electron_acceleration_multiplier,
+                      bfield=p.elliptic.magnetic_field, kappa=p.elliptic.poisson_coefficient,
+                      courant=p.stepper.courant)
+    ctx.set_background(None)
+    rng = np.random.default_rng(900 + res[2])
+    f = rng.standard_normal(c.shape).astype(np.float32).astype(np.float64)
+    E = rng.standard_normal((res[0] + 2, n))
+    tf = torch.as_tensor(f, dtype=torch.float32, device="cuda")
+    tE = torch.as_tensor(E, device="cuda")
+    J = (c.x.J, c.u.J, c.v.J)
+    parts = []
+    for d in range(3):
+        w = [0.0, 0.0, 0.0]
+        w[d] = J[d]
+        out = torch.zeros_like(tf)
+        ctx.rhs_weighted(tf, tE, out, w, xhalo=_lib.VL_XHALO_GHOST)
+        parts.append(out.cpu().numpy().astype(np.float64)[INNER])
+    R = vo.rhs(f, E, c)[INNER]
+    assert rel_err(parts[0] + parts[1] + parts[2], R) < 1e-5
+    for part in parts:
+        assert np.max(np.abs(part)) > 1e-3 * np.max(np.abs(R))

@@ -48,7 +48,8 @@ def test_mlp_gradients_against_oracle(cuda):
         err = np.linalg.norm(g - dW[l]) / np.linalg.norm(dW[l])
         errb = np.linalg.norm(gb[l] - db[l]) / np.linalg.norm(db[l])
         print(f"layer {l}: dW normwise {err:.2e}, db {errb:.2e}")
-        assert err < 1e-2 and errb < 1e-2
+        # measured up to 1.3e-4 (dW) on a B200: the bar keeps an 8x margin
+        assert err < 1e-3 and errb < 1e-3
 
 
 def test_training_fits_a_smooth_map(cuda):
@@ -114,3 +115,40 @@ def test_trained_closure_gains_over_plain_coarse_rhs(cuda):
     after = evaluate(mlp, Xva, Tva)
     print(f"held-out RHS error: plain coarse {zero:.3e}, with closure {after:.3e}")
     assert after < 0.8 * zero
+
+
+def test_charge_conserving_correction(cuda):
+    """vl_closure_apply in its charge-conserving mode: a random network output applied to a zero
+    state leaves the zeroth moment (the charge density the field is solved from) at zero, while
+    the plain mode with the same output changes it; both modes agree up to the removed mean."""
+    import ctypes
+
+    from vlasov1d2v_b200 import _device, _lib, problem
+    from vlasov1d2v_b200.closure import CN, OUT
+
+    p = problem.build((3, 4, 5), 6, perturbation=None, amp=0.0)
+    nx, nu, nv = 3, 4, 5
+    ns = nx * CN * nu * nv
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    Y = torch.randn((ns, OUT), device="cuda", generator=g)
+    sc = torch.rand(ns, device="cuda", generator=g) + 0.5
+    dt = torch.tensor([0.01], dtype=torch.float64, device="cuda")
+    w = (ctypes.c_double * CN)(*[float(x) for x in p.basis.b1.weights])
+    wp = ctypes.cast(w, ctypes.POINTER(ctypes.c_double))
+    rho = {}
+    outs = {}
+    for mode in (_lib.VL_CLOSURE_PLAIN, _lib.VL_CLOSURE_CHARGE):
+        out = torch.zeros(p.f.arr.shape, dtype=torch.float64, device="cuda")
+        _lib.call("vl_closure_apply", ctypes.c_void_p(out.data_ptr()), _lib.VL_FP64, nx, nu, nv,
+                  ctypes.c_void_p(Y.data_ptr()), ctypes.c_void_p(sc.data_ptr()), 2.0, 1e30,
+                  ctypes.c_void_p(dt.data_ptr()), 0.5, None, mode, wp, ctypes.c_void_p(_device.stream_handle()))
+        rho[mode] = p.f.moment_zero_of_arr(out).get()
+        outs[mode] = out.cpu().numpy()
+    scale = np.max(np.abs(outs[_lib.VL_CLOSURE_PLAIN]))
+    assert np.max(np.abs(rho[_lib.VL_CLOSURE_CHARGE])) < 1e-13 * scale
+    assert np.max(np.abs(rho[_lib.VL_CLOSURE_PLAIN])) > 1e-4 * scale
+    # the difference of the two modes is constant over the velocity nodes of each x node
+    d = (outs[_lib.VL_CLOSURE_PLAIN] - outs[_lib.VL_CLOSURE_CHARGE])[1:-1, :, 1:-1, :, 1:-1, :]
+    d = d.reshape(nx, CN, -1)
+    assert np.max(np.abs(d - d[:, :, :1])) < 1e-13 * scale

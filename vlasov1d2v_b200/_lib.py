@@ -31,6 +31,8 @@ EXPORTED = (
     "vl_poisson_dg", "vl_axpby_interior",
 )
 NOALLOC_SCRATCH_BYTES = 1 << 20
+VL_CLOSURE_PLAIN = 0
+VL_CLOSURE_CHARGE = 1
 VL_ENS_NATIVE_AUTO = 0xFFFFFFFF
 
 _c_dbl_p = ctypes.POINTER(ctypes.c_double)
@@ -123,7 +125,7 @@ def _declare(lib):
     lib.vl_mlp_backward.argtypes = [vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.vl_mlp_adam.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, f32, vp]
     lib.vl_closure_features.argtypes = [vp, i32, i32, i32, i32, vp, f64, f64, vp, vp, f64, f64, f64, vp, vp, vp]
-    lib.vl_closure_apply.argtypes = [vp, i32, i32, i32, i32, vp, vp, f64, f32, vp, f64, vp, vp]
+    lib.vl_closure_apply.argtypes = [vp, i32, i32, i32, i32, vp, vp, f64, f32, vp, f64, vp, i32, vp, vp]
     lib.vl_initial_state.argtypes = [vp, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp, vp,
                                      ctypes.c_double, vp]
     lib.vl_smooth_edges.argtypes = [vp, i32, i32, i32, i32, i32, vp]

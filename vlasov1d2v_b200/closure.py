@@ -302,14 +302,20 @@ class ClosureStepper:
     ``mlp=None`` runs the plain coarse operator through the same loop.  One step is a fixed
     sequence of device launches (native kernels + a few torch reductions), CUDA-graph captured."""
 
-    def __init__(self, coarse, mlp=None, escale=1.0, alpha=1.0):
-        """``alpha`` scales the learned correction (1: as trained; below 1: relaxed)."""
+    def __init__(self, coarse, mlp=None, escale=1.0, alpha=1.0, constraint=None):
+        """``alpha`` scales the learned correction (1: as trained; below 1: relaxed).
+        ``constraint="charge"`` removes, per x node, the quadrature mean of the correction over
+        velocity, so the closure cannot change the charge density that drives the field."""
         from .context import get_context
 
         self.p = coarse
         self.mlp = mlp
         self.escale = float(escale)
         self.alpha = float(alpha)
+        if constraint not in (None, "charge"):
+            raise ValueError("constraint must be None or 'charge'")
+        self.mode = _lib.VL_CLOSURE_CHARGE if constraint == "charge" else _lib.VL_CLOSURE_PLAIN
+        self._node_w = (ctypes.c_double * CN)(*[float(w) for w in coarse.basis.b1.weights])
         g = coarse.grids
         self.ctx = get_context(g, precision="fp64", accel=coarse.refs.electron_acceleration_multiplier,
                                bfield=coarse.elliptic.magnetic_field, kappa=coarse.elliptic.poisson_coefficient,
@@ -354,7 +360,7 @@ class ClosureStepper:
         self.mlp.forward(self.X, self.Y)
         _lib.call("vl_closure_apply", _vp(out), _lib.VL_FP64, self.nx, g.u.res, g.v.res, _vp(self.Y),
                   _vp(self.sc), self.cscale, float(self.mlp.ymax), _vp(self.dt), float(c2 * self.alpha), None,
-                  _stream())
+                  int(self.mode), ctypes.cast(self._node_w, ctypes.POINTER(ctypes.c_double)), _stream())
 
     def _step(self, k):
         f, sa, sb = self.f, self.sa, self.sb

@@ -78,6 +78,8 @@ def main(argv=None):
     ap.add_argument("--coarse-res", type=int, nargs=3, default=[16, 20, 20])
     ap.add_argument("--alpha", type=float, nargs="+", default=[1.0],
                     help="scales of the learned correction to run (1: as trained)")
+    ap.add_argument("--constraint", nargs="+", default=["none"], choices=["none", "charge"],
+                    help="forms of the correction to run: as predicted, or charge-conserving")
     args = ap.parse_args(argv)
     fine_res, coarse_res = tuple(args.fine_res), tuple(args.coarse_res)
     escale = 0.05
@@ -161,15 +163,17 @@ def main(argv=None):
                 "fine_steps": int(fine.stepper.steps_counter), "coarse_steps": int(nsteps),
                 "plain": score(plain.stepper.time_array, plain.stepper.field_energy, plain.f.arr)})
     runs = []
-    for alpha in args.alpha:
-        _, cl = _problems(q, fine_res, coarse_res)
-        cs = ClosureStepper(cl, mlp=mlp, escale=escale, alpha=alpha)
-        sec = _timed(lambda: cs.run_steps(nsteps, batch=50))
-        rec = {"alpha": alpha, "closure_s": sec, "fallback_step": cs.fallback_step,
-               "speedup_vs_fine": out["fine_s"] / sec, **score(cs.times, cs.energies, cl.f.arr)}
-        _log(rec)
-        runs.append(rec)
-        del cs, cl
+    for constraint in args.constraint:
+        for alpha in args.alpha:
+            _, cl = _problems(q, fine_res, coarse_res)
+            cs = ClosureStepper(cl, mlp=mlp, escale=escale, alpha=alpha,
+                                constraint=None if constraint == "none" else constraint)
+            sec = _timed(lambda: cs.run_steps(nsteps, batch=50))
+            rec = {"alpha": alpha, "constraint": constraint, "closure_s": sec, "fallback_step": cs.fallback_step,
+                   "speedup_vs_fine": out["fine_s"] / sec, **score(cs.times, cs.energies, cl.f.arr)}
+            _log(rec)
+            runs.append(rec)
+            del cs, cl
     out["closure_runs"] = runs
     # the first run under the earlier keys
     first = runs[0]

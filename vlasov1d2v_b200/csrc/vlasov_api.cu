@@ -306,6 +306,8 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             if constexpr (sizeof(T) == 4) {
                 // FP32: the packed-FMA kernel, one instantiation per stage kind and background split
                 a.usv = c->d_usv4;
+                a.sx = a.jx / c->cfg.jx;
+                a.sv = a.jv / c->cfg.jv;
                 const vl::F32Tables &ft = f32_tables(c);
                 const bool bg = a.bg_rb != nullptr;
                 const dim3 blk(G::THREADS);

@@ -68,6 +68,10 @@ struct StageArgs {
     // tables in the velocity-slab layout [U][n][V][n] (index a sA + j sJ + v column).
     const float *bg_rb;
     const float *bg_eu;
+    // FP32 n = 8 kernel: its per-u-node speed table holds u J_x and a (-B u) J_v with the
+    // context's Jacobians; a call with other direction weights (jx, jv above) scales them by
+    // jx / J_x and jv / J_v (the RHS kind only; the RK stages use the context's Jacobians)
+    double sx, sv;
 };
 
 

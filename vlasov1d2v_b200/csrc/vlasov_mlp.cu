@@ -460,6 +460,60 @@ __global__ void closure_apply_kernel(T *__restrict__ out, int nx, int nu, int nv
     }
 }
 
+// Charge-conserving form: one CTA per x node (e, i) removes from the correction of that node the
+// quadrature mean over all of its velocity nodes, so the correction leaves the zeroth moment -- the
+// charge density the field is solved from -- unchanged:
+//   c[s, j, k] = scale[s] clamp(Y[s][6 j + k]),  mean = sum w_j w_k c / sum w_j w_k,
+//   out += c2 dt cscale (c - mean)
+struct NodeWeights {
+    double w[CN];
+};
+
+constexpr int CONS_THREADS = 256;
+
+template <typename T>
+__global__ void __launch_bounds__(CONS_THREADS)
+closure_apply_conservative_kernel(T *__restrict__ out, int nx, int nu, int nv, const float *__restrict__ Y,
+                                  const float *__restrict__ scale, double cscale, float ymax,
+                                  const double *__restrict__ dt, double c2, const vl_run_state *__restrict__ state,
+                                  const NodeWeights wq) {
+    __shared__ double s_part[CONS_THREADS / 32];
+    if (state != nullptr && state->active == 0) return;
+    const int node = blockIdx.x;   // e CN + i, e 0-based
+    const int e = node / CN + 1, i = node % CN;
+    const int U = nu + 2, V = nv + 2;
+    const long sJ = (long)V * CN, sA = sJ * CN, sI = sA * U, sE = sI * CN;
+    const long nsamp = (long)nu * nv;
+    const long s0 = (long)node * nsamp;
+    const long count = nsamp * CN * CN;
+    double acc = 0.0;
+    for (long q = threadIdx.x; q < count; q += blockDim.x) {
+        const long s = s0 + q / (CN * CN);
+        const int jk = (int)(q % (CN * CN));
+        const float y = fminf(fmaxf(Y[s * OUT + jk], -ymax), ymax);
+        acc = fma(wq.w[jk / CN] * wq.w[jk % CN], (double)scale[s] * (double)y, acc);
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    double tot = 0.0, wsum = 0.0;
+    for (int w = 0; w < CONS_THREADS / 32; ++w) tot += s_part[w];
+    for (int j = 0; j < CN; ++j)
+        for (int k = 0; k < CN; ++k) wsum += wq.w[j] * wq.w[k];
+    const double mean = tot / (wsum * (double)nsamp);
+    const double w = c2 * (*dt) * cscale;
+    for (long q = threadIdx.x; q < count; q += blockDim.x) {
+        const long s = s0 + q / (CN * CN);
+        const int jk = (int)(q % (CN * CN));
+        const int j = jk / CN, k = jk % CN;
+        const long sl = s - s0;
+        const int a = (int)(sl / nv) + 1, b = (int)(sl % nv) + 1;
+        const long o = e * sE + i * sI + a * sA + j * sJ + b * CN + k;
+        const float y = fminf(fmaxf(Y[s * OUT + jk], -ymax), ymax);
+        out[o] = (T)((double)out[o] + w * ((double)scale[s] * (double)y - mean));
+    }
+}
+
 MlpWeights weights_of(const __nv_bfloat16 *wf, const __nv_bfloat16 *wb, const float *bias) {
     MlpWeights w;
     for (int l = 0; l < NL; ++l) {
@@ -508,9 +562,23 @@ VL_API int vl_closure_features(const void *f, int32_t prec, int32_t nx, int32_t 
 
 VL_API int vl_closure_apply(void *out, int32_t prec, int32_t nx, int32_t nu, int32_t nv, const float *Y,
                             const float *scale, double cscale, float ymax, const double *dt, double c2,
-                            const vl_run_state *state, void *stream) {
+                            const vl_run_state *state, int32_t mode, const double *node_weights, void *stream) {
     if (!out || !Y || !scale || !dt) return fail(VL_ERR_INVALID, "null argument");
+    if (mode != VL_CLOSURE_PLAIN && mode != VL_CLOSURE_CHARGE) return fail(VL_ERR_INVALID, "closure mode");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (mode == VL_CLOSURE_CHARGE) {
+        if (!node_weights) return fail(VL_ERR_INVALID, "null node weights");
+        NodeWeights wq;
+        for (int j = 0; j < CN; ++j) wq.w[j] = node_weights[j];
+        const int blocks = nx * CN;
+        if (prec == VL_FP64)
+            closure_apply_conservative_kernel<double><<<blocks, CONS_THREADS, 0, s>>>(
+                static_cast<double *>(out), nx, nu, nv, Y, scale, cscale, ymax, dt, c2, state, wq);
+        else
+            closure_apply_conservative_kernel<float><<<blocks, CONS_THREADS, 0, s>>>(
+                static_cast<float *>(out), nx, nu, nv, Y, scale, cscale, ymax, dt, c2, state, wq);
+        return check("closure_apply_conservative_kernel");
+    }
     const long total = (long)nx * CN * nu * nv * CN * CN;
     const int blocks = (int)((total + 255) / 256 < 148 * 32 ? (total + 255) / 256 : 148 * 32);
     if (prec == VL_FP64)

@@ -138,6 +138,7 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
     const float2 dt2 = f2s((float)dtd), c12 = f2s((float)a.c1), c2dt2 = f2s((float)(a.c2 * dtd));
     const float2 mone = f2s(-1.0f);
     const float ju = (float)a.ju;
+    const float rsx = (float)a.sx, rsv = (float)a.sv;
     const double Ei = a.E[Eg * N + g];
     const float2 Ei2 = f2s((float)Ei);
     // per-thread coefficients: x rows g (pairs), v rows k0, k1 (pairs over m), both upwind variants
@@ -227,8 +228,14 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
                 if constexpr (UNI) set_dirs(us0.x >= 0.0f, us0.z >= 0.0f);
 #pragma unroll
                 for (int j = 0; j < N; ++j) {
-                    const float4 us = sUS[j];   // {u J_x, u J_x, a (-B u) J_v, a (-B u) J_v}
+                    float4 us = sUS[j];   // {u J_x, u J_x, a (-B u) J_v, a (-B u) J_v}
                     if constexpr (!UNI) set_dirs(us.x >= 0.0f, us.z >= 0.0f);
+                    if constexpr (KIND == KIND_RHS) {   // caller-chosen direction weights
+                        us.x *= rsx;
+                        us.y *= rsx;
+                        us.z *= rsv;
+                        us.w *= rsv;
+                    }
                     // x: sum_m up[g][m] F[m][j][k, k+1] with the own trace folded, + neighbour trace
                     const float *pc = sIn + j * W + P + cl;
                     float2 dx = fmul2(cx[0], lds2(pc));
