@@ -60,8 +60,9 @@ def parse():
 
 
 def kernel_only(args):
-    """Plain launches of the three fused stage kinds and one field solve (no graphs, no timing
-    of its own): the target of ncu captures of single kernels."""
+    """Plain launches of the three fused stage kinds, the standalone moment and one field solve
+    per repetition (no graphs, no timing of its own): the target of ncu captures of single
+    kernels."""
     import torch
 
     from vlasov1d2v_b200 import problem
@@ -84,10 +85,15 @@ def kernel_only(args):
         # the FP32 mixed form's stage kernels also read the background RHS tables
         ctx.set_background(p.f.background_tables(p.grids, p.refs.electron_acceleration_multiplier,
                                                  p.elliptic.magnetic_field))
+    rho = torch.zeros((res[0], n), dtype=torch.float64, device=f.device)
+    phi = torch.empty_like(rho)
     for _ in range(args.kernel_reps):
         ctx.rk_stage(0, f, None, sa, E, dt, partials=ctx.workspace)
         ctx.rk_stage(1, sa, f, sb, E, dt, partials=ctx.workspace)
         ctx.rk_stage(2, sb, f, sa, E, dt, partials=ctx.workspace)
+        # the standalone moment and the single-CTA field solve of the same problem
+        ctx.moment(f, rho)
+        ctx.poisson((rho.mean() - rho).contiguous(), E, phi)
     torch.cuda.synchronize()
     print(json.dumps({"kernel_only": True, "res": list(res), "order": n, "precision": args.precision,
                       "reps": args.kernel_reps,

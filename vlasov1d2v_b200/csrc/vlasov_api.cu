@@ -286,7 +286,7 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
         }
     vl::StageArgs a = a0;
     if (a.err == nullptr) a.err = c->d_err;
-    dim3 grid(c->stage_grid_g, c->cfg.nx);
+    dim3 grid(a.kind == vl::KIND_COMBINE ? c->stage_grid_g : c->stage_grid_g1, c->cfg.nx);
     if constexpr (N == 8) {
         if (c->use_frag) {
             using G = vl::FragGeom<T>;
@@ -330,8 +330,15 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                 }
                 return check_launch(le, "stage_f32_kernel");
             } else {
-                return check_launch(launch(c, vl::stage_frag_kernel<T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
-                                           tb, maps),
+                // FP64: combination stages stage an f^n tile; Euler / RHS stages take the form
+                // without it (3 CTAs per SM)
+                if (a.kind == vl::KIND_COMBINE)
+                    return check_launch(launch(c, vl::stage_frag_kernel<T, true>, grid, dim3(G::THREADS),
+                                               G::smem_bytes(), s, a, tb, maps),
+                                        "stage_frag_kernel");
+                using G1 = vl::FragGeom<T, false>;
+                return check_launch(launch(c, vl::stage_frag_kernel<T, false>, grid, dim3(G1::THREADS),
+                                           G1::smem_bytes(), s, a, tb, maps),
                                     "stage_frag_kernel");
             }
         }
@@ -451,9 +458,9 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
                                                                   G::THREADS, smem) != cudaSuccess)
                     return 1;
             } else {
-                cudaFuncSetAttribute(vl::stage_frag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                cudaFuncSetAttribute(vl::stage_frag_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T>,
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T, true>,
                                                                   G::THREADS, smem) != cudaSuccess)
                     return 1;
             }
@@ -478,6 +485,19 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_pencil_kernel<N, T>,
                                                       G::THREADS, smem) != cudaSuccess)
+        return 1;
+    return blocks > 0 ? blocks : 1;
+}
+
+// resident CTAs per SM of the FP64 n = 8 fragment kernel's form without the f^n tile
+int frag_nofn_occupancy() {
+    using G = vl::FragGeom<double, false>;
+    const size_t smem = G::smem_bytes();
+    cudaFuncSetAttribute(vl::stage_frag_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<double, false>, G::THREADS,
+                                                      smem) != cudaSuccess)
         return 1;
     return blocks > 0 ? blocks : 1;
 }
@@ -620,7 +640,8 @@ int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
 
 // bytes of the moment partials inside a loop workspace
 size_t partials_bytes(const vl_ctx *c) {
-    const int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
+    int g = c->stage_grid_g > c->moment_grid_g ? c->stage_grid_g : c->moment_grid_g;
+    if (c->stage_grid_g1 > g) g = c->stage_grid_g1;
     const size_t b = sizeof(double) * (size_t)c->cfg.nx * g * c->cfg.n;
     return (b + 255) & ~(size_t)255;
 }
@@ -848,10 +869,15 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double
     // the kernel time)
-    int g = (c->sm_count * occ) / cfg->nx;
-    if (g > tiles) g = tiles;
-    if (g < 1) g = 1;
-    c->stage_grid_g = g;
+    auto grid_for = [&](int o) {
+        int g = (c->sm_count * o) / cfg->nx;
+        if (g > tiles) g = tiles;
+        if (g < 1) g = 1;
+        return g;
+    };
+    c->stage_grid_g = grid_for(occ);
+    c->stage_grid_g1 = (c->use_frag && cfg->precision == VL_FP64) ? grid_for(frag_nofn_occupancy())
+                                                                  : c->stage_grid_g;
     // standalone moment: MOMENT_CTAS_PER_SM resident CTAs per SM, at most one per u element
     int gm = (c->sm_count * vl::MOMENT_CTAS_PER_SM) / cfg->nx;
     if (gm > cfg->nu) gm = cfg->nu;
@@ -1056,7 +1082,6 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
         fa.mode = vl::FIELD_PROMOTE;
         fa.phi = nullptr;
         if ((rc = field(c, fa, s))) return rc;
-        fa.G = G;   // from here on the partials come from the stage kernels
         st.in = f;
         st.fn = nullptr;
         st.out = sa;
@@ -1065,6 +1090,7 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
         if ((rc = stage(c, st, s))) return rc;
         // stage 1: E(s0); s1 = 3/4 f + 1/4 s0 + 1/4 dt R(s0)
         fa.mode = vl::FIELD_REQUIRE_ACTIVE;
+        fa.G = c->stage_grid_g1;   // partials of the Euler stage's grid
         if ((rc = field(c, fa, s))) return rc;
         st.in = sa;
         st.fn = f;
@@ -1079,6 +1105,7 @@ int vl_ssp_rk3_steps(vl_ctx *c, void *f, void *sa, void *sb, double *E, double *
         //          f <- 1/3 f + 2/3 s1 + 2/3 dt R(s1)
         fa.mode = vl::FIELD_REQUIRE_ACTIVE | vl::FIELD_RECORD;
         fa.phi = phi;
+        fa.G = G;                  // from here on the partials of the combination stages' grid
         if ((rc = field(c, fa, s))) return rc;
         st.in = sb;
         st.fn = f;

@@ -19,6 +19,8 @@ struct vl_ctx {
     int device;
     int sm_count;
     int stage_grid_g;   // CTAs per x element of the stage kernel (moment partials per e)
+    int stage_grid_g1;  // the same for the Euler and RHS stages (FP64 n = 8: a form without the
+                        // f^n tile that fits more CTAs per SM; elsewhere = stage_grid_g)
     int moment_grid_g;  // CTAs per x element of the standalone moment kernel
     double up[vl::NMAX * vl::NMAX];
     double xi[vl::NMAX * 2];

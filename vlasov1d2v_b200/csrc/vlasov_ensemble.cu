@@ -465,6 +465,9 @@ int commit(vl_ens *E) {
             }
         E->members[i].G = G;
         for (int k = 0; k < 3; ++k) E->field[k][i].G = G;
+        // a member launched through its own context: the solve after the Euler stage reads the
+        // partials of that context's Euler-stage grid
+        if (E->by_order && E->native[i]) E->field[1][i].G = c->stage_grid_g1;
         E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes));
     }
     std::vector<int> offs;

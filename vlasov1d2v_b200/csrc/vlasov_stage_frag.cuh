@@ -52,7 +52,9 @@
 
 namespace vl {
 
-template <typename T>
+// WFN: the stage holds an f^n tile (combination stages); without it (Euler and RHS stages) an FP64
+// CTA needs 58 KB of shared memory instead of 97 KB, so three CTAs fit an SM
+template <typename T, bool WFN = true>
 struct FragGeom {
     static constexpr int N = 8;
     static constexpr int EPT = 4;                    // v elements per tile (one per warp)
@@ -67,10 +69,10 @@ struct FragGeom {
     static constexpr int NJ = N / JS;                // j rows per warp
     static constexpr int THREADS = 32 * EPT * JS;
     static constexpr bool MMA = sizeof(T) == 8;      // tensor-core x/v contractions (FP64)
-    static constexpr int MINB = sizeof(T) == 8 ? VL_FRAG_MINB64 : VL_FRAG_MINB32;   // CTAs per SM
+    static constexpr int MINB = sizeof(T) == 8 ? (WFN ? VL_FRAG_MINB64 : 3) : VL_FRAG_MINB32;   // CTAs per SM
     static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
     static constexpr size_t IN_B = al(sizeof(T) * (size_t)PS * N);
-    static constexpr size_t FN_B = al(sizeof(T) * (size_t)PSF * N);
+    static constexpr size_t FN_B = WFN ? al(sizeof(T) * (size_t)PSF * N) : 0;
     static constexpr size_t XF_B = al(sizeof(T) * (size_t)2 * COLS * N);
     static constexpr size_t UF_B = XF_B;
     // background-split RHS tables (a form of the FP32 context only)
@@ -113,11 +115,11 @@ struct Pair<float> {
     using V = float2;
 };
 
-template <typename T>
-__global__ void __launch_bounds__(FragGeom<T>::THREADS, FragGeom<T>::MINB)
+template <typename T, bool WFN>
+__global__ void __launch_bounds__(FragGeom<T, WFN>::THREADS, FragGeom<T, WFN>::MINB)
 stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                   const __grid_constant__ FragMaps maps) {
-    using G = FragGeom<T>;
+    using G = FragGeom<T, WFN>;
     using V2 = typename Pair<T>::V;
     constexpr int N = G::N, P = G::P, W = G::W, PS = G::PS, WF = G::WF, PSF = G::PSF;
     constexpr int COLS = G::COLS, EPT = G::EPT, NT = G::THREADS;
@@ -153,7 +155,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         Er = e + 2;
     }
     const int kind = a.kind;
-    const bool with_fn = (kind == KIND_COMBINE);
+    const bool with_fn = WFN && (kind == KIND_COMBINE);   // combination stages launch the WFN form
     const bool with_bg = G::BG && a.bg_rb != nullptr;
     const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0) +
                               (uint32_t)(2 * sizeof(T)) * N;
@@ -384,10 +386,12 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     } else if (kind == KIND_EULER) {
                         o.x = fma(dtT, r0, fij.x);
                         o.y = fma(dtT, r1, fij.y);
-                    } else {
+                    } else if constexpr (WFN) {
                         const V2 fnv = *reinterpret_cast<const V2 *>(sFn + g * PSF + j * WF + P + cl);
                         o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
                         o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
+                    } else {
+                        o = fij;   // not reached: combination stages launch the WFN form
                     }
                     *reinterpret_cast<V2 *>(pout + j * sJ) = o;
                     if (gout != nullptr) {
