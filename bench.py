@@ -254,12 +254,16 @@ class Clocks:
 # ----------------------------------------------------------------------------------------------
 # GPU measurement
 # ----------------------------------------------------------------------------------------------
+STAGE_PROFILES = {"fp64": "stage_frag_fp64_16x50x50_n8.md", "fp32": "stage_f32_fp32_16x50x50_n8.md"}
+
+
 def profiled_traffic_ratio(precision):
     """DRAM bytes (read + write) per algorithmic byte of one fused stage launch, from the ncu
-    capture summarised in profiles/stage_frag_<precision>_16x50x50_n8.md (a half-size case of
-    the same kernel; the traffic scales with the elements processed).  None when absent."""
+    capture summarised in profiles/ for the benchmark's stage kernel of that precision (a
+    half-size case of the same kernel; the traffic scales with the elements processed).  None
+    when absent."""
     import re
-    path = os.path.join(ROOT, "profiles", f"stage_frag_{precision}_16x50x50_n8.md")
+    path = os.path.join(ROOT, "profiles", STAGE_PROFILES[precision])
     try:
         text = open(path).read()
     except OSError:
@@ -558,8 +562,8 @@ def main():
                    "buffers, 3 buffers)", "parallelism": f"replicas x{world}"},
         "roofline": head["roofline"],
         "e2e": head["e2e"],
-        # per step: 3 fused stage kernels + 3 field solves of 2 kernels; one moment per call
-        "gpu_launches": 9 * args.steps + 1,
+        # per step: 3 fused stage kernels + 3 single-CTA field solves; one moment per call
+        "gpu_launches": 6 * args.steps + 1,
         "clocks": ck,
         "variants": {"fp32_mixed": {"value": out["fp32"]["value"], "dtype": "f32",
                                     "ms_per_step": out["fp32"]["ms_per_step"],
