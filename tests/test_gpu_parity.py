@@ -133,7 +133,9 @@ def test_steps_match_reference_energy_1e12(cuda, name):
     nst = len(G["energy"]) - 1
     p.stepper.run_steps(p.f, p.basis, p.elliptic, p.grids, p.flux, p.refs, nst)
     np.testing.assert_allclose(p.stepper.field_energy, G["energy"], rtol=F_RTOL, atol=0)
-    np.testing.assert_allclose(p.stepper.time_array, G["time"], rtol=1e-14, atol=0)
+    # dt (hence the clock) follows max |a E|, which dominates the speeds at this amplitude and
+    # carries the field's rounding (measured 2.8e-14 at n = 8)
+    np.testing.assert_allclose(p.stepper.time_array, G["time"], rtol=1e-13, atol=0)
     assert rel_err(_np(p.f.arr)[INNER], G[f"f_step{nst}"]) < F_RTOL
     assert rel_err(_np(p.elliptic.electric_field), G[f"E_step{nst}"]) < F_RTOL
 

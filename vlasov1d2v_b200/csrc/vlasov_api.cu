@@ -613,6 +613,7 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     a.ell = c->d_ell;
     a.phase = c->d_phase;
     a.qnode = c->d_qnode;
+    a.stage_phase = vl::field_stage_phase(c->cfg.n, c->cfg.n_modes, c->cfg.nx) ? 1 : 0;
     a.k = c->d_k;
     a.xw = c->d_xw;
     a.nx = c->cfg.nx;
@@ -634,7 +635,8 @@ vl::FieldArgs field_args(const vl_ctx *c) {
 // the whole spectral solve in one CTA (vlasov_field.cuh)
 int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
     return check_launch(launch(c, vl::field_solve_kernel, dim3(1), dim3(vl::FS_THREADS),
-                               vl::field_solve_smem(c->cfg.n, c->cfg.n_modes), s, a),
+                               vl::field_solve_smem(c->cfg.n, c->cfg.n_modes, c->cfg.nx, a.stage_phase != 0), s,
+                               a),
                         "field_solve_kernel");
 }
 
@@ -798,7 +800,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if ((rc = upload(&c->d_qnode, cfg->dft_qnode, nm))) return cleanup(rc);
     {
         const cudaError_t ee = cudaFuncSetAttribute(vl::field_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
+                                                    (int)vl::FS_DYN_MAX);
         if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaFuncSetAttribute(field_solve_kernel)"));
     }
     {

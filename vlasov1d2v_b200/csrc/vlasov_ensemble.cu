@@ -468,7 +468,9 @@ int commit(vl_ens *E) {
         // a member launched through its own context: the solve after the Euler stage reads the
         // partials of that context's Euler-stage grid
         if (E->by_order && E->native[i]) E->field[1][i].G = c->stage_grid_g1;
-        E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes));
+        const bool staged = vl::field_stage_phase(c->cfg.n, c->cfg.n_modes, c->cfg.nx);
+        for (int k = 0; k < 3; ++k) E->field[k][i].stage_phase = staged ? 1 : 0;
+        E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes, c->cfg.nx, staged));
     }
     std::vector<int> offs;
     std::vector<vl::EnsItem> flat;
@@ -560,7 +562,7 @@ VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     cudaFuncSetAttribute(vl::ens_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
+                         (int)vl::FS_DYN_MAX);
     *out = E;
     return VL_OK;
 }

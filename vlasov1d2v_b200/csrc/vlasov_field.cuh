@@ -27,8 +27,17 @@ constexpr int FS_THREADS = 1024;
 constexpr int FS_FWD_PARTS = 3;    // element ranges per mode (M <= 321 -> 963 threads)
 constexpr int FS_INV_PARTS = 4;    // mode ranges per node (256 nodes per pass)
 
-// dynamic shared memory of the solve: C_E and C_P, [n][M] complex each
-__host__ __device__ constexpr size_t field_solve_smem(int n, int M) { return 2 * sizeof(double2) * (size_t)n * M; }
+// dynamic shared memory of the solve: C_E and C_P, [n][M] complex each, then (staged) the
+// element phases [nx][M]; the largest dynamic size a launch may ask for (static ~33 KB beside it)
+constexpr size_t FS_DYN_MAX = 190 * 1024;
+__host__ __device__ constexpr size_t field_solve_smem(int n, int M, int nx, bool staged) {
+    return sizeof(double2) * ((size_t)2 * n * M + (staged ? (size_t)nx * M : 0));
+}
+// whether a problem's element phases are staged in shared memory (every grid with nx M small
+// enough: all benchmark grids up to nx = 32)
+__host__ __device__ constexpr bool field_stage_phase(int n, int M, int nx) {
+    return field_solve_smem(n, M, nx, true) <= FS_DYN_MAX;
+}
 
 __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
     __shared__ double s_rho[FIELD_MAX_NODES];                  // rho, then rhs, then E
@@ -45,16 +54,24 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
     const int n = a.n, nx = a.nx, nn = nx * n, M = a.M;
     double2 *sCE = fs_dyn;
     double2 *sCP = fs_dyn + (size_t)n * M;
+    // the element phases are read by every thread of the forward and inverse loops: copied once
+    // into shared memory (coalesced, all threads) while the charge is formed, so the loops do not
+    // wait on one global load per mode
+    double2 *sPH = fs_dyn + (size_t)2 * n * M;
+    if (a.stage_phase)
+        for (int q = tid; q < nx * M; q += blockDim.x) sPH[q] = a.phase[q];
+    const double2 *PH = a.stage_phase ? sPH : a.phase;
 
     // 1. charge
     if (a.charge_in != nullptr) {
         for (int p = tid; p < nn; p += blockDim.x) s_rho[p] = a.kappa * a.charge_in[p];
-        __syncthreads();
+        __syncthreads();   // also publishes the staged phases
     } else {
         double loc = 0.0, locc = 0.0;
         for (int p = tid; p < nn; p += blockDim.x) {
             const int e = p / n, i = p - e * n;
             dd sacc = {0.0, 0.0};
+#pragma unroll 8
             for (int gg = 0; gg < a.G; ++gg) sacc = dd_add(sacc, dd{a.partials[((size_t)e * a.G + gg) * n + i], 0.0});
             const double rho = sacc.hi + sacc.lo;
             s_rho[p] = rho;
@@ -77,6 +94,7 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
             for (int j = 0; j < NMAX; ++j) ell[j] = (j < n) ? a.ell[(size_t)j * M + m] : make_double2(0.0, 0.0);
             const int e0 = (part * nx) / FS_FWD_PARTS, e1 = ((part + 1) * nx) / FS_FWD_PARTS;
             double cr = 0.0, ci = 0.0;
+#pragma unroll 2
             for (int e = e0; e < e1; ++e) {
                 double sr = 0.0, si = 0.0;
 #pragma unroll
@@ -87,7 +105,7 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
                         si = fma(r, ell[j].y, si);
                     }
                 }
-                const double2 ph = a.phase[(size_t)e * M + m];
+                const double2 ph = PH[(size_t)e * M + m];
                 cr = fma(ph.x, sr, fma(-ph.y, si, cr));
                 ci = fma(ph.x, si, fma(ph.y, sr, ci));
             }
@@ -139,9 +157,10 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
         double er = 0.0, pr = 0.0;
         if (p < nn) {
             const int e = p / n, j = p - e * n;
-            const double2 *ph = a.phase + (size_t)e * M;
+            const double2 *ph = PH + (size_t)e * M;
             const double2 *ce = sCE + (size_t)j * M;
             const double2 *cp = sCP + (size_t)j * M;
+#pragma unroll 4
             for (int m = part; m < M; m += FS_INV_PARTS) {
                 const double2 h = ph[m];   // Re(conj(h) c) = h.x c.x + h.y c.y
                 er = fma(h.x, ce[m].x, fma(h.y, ce[m].y, er));
