@@ -613,7 +613,6 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     a.ell = c->d_ell;
     a.phase = c->d_phase;
     a.qnode = c->d_qnode;
-    a.stage_phase = vl::field_stage_phase(c->cfg.n, c->cfg.n_modes, c->cfg.nx) ? 1 : 0;
     a.k = c->d_k;
     a.xw = c->d_xw;
     a.nx = c->cfg.nx;
@@ -632,12 +631,22 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     return a;
 }
 
-// the whole spectral solve in one CTA (vlasov_field.cuh)
+// the whole spectral solve in one thread-block cluster of vl::FC CTAs (vlasov_field.cuh)
 int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
-    return check_launch(launch(c, vl::field_solve_kernel, dim3(1), dim3(vl::FS_THREADS),
-                               vl::field_solve_smem(c->cfg.n, c->cfg.n_modes, c->cfg.nx, a.stage_phase != 0), s,
-                               a),
-                        "field_solve_kernel");
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(vl::FC);
+    cfg.blockDim = dim3(vl::FS_THREADS);
+    cfg.dynamicSmemBytes = vl::field_solve_smem(c->cfg.n, c->cfg.n_modes);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = vl::FC;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return check_launch(cudaLaunchKernelEx(&cfg, vl::field_solve_kernel, a), "field_solve_kernel");
 }
 
 // bytes of the moment partials inside a loop workspace
@@ -800,7 +809,7 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     if ((rc = upload(&c->d_qnode, cfg->dft_qnode, nm))) return cleanup(rc);
     {
         const cudaError_t ee = cudaFuncSetAttribute(vl::field_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)vl::FS_DYN_MAX);
+                                                    (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
         if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaFuncSetAttribute(field_solve_kernel)"));
     }
     {

@@ -198,9 +198,9 @@ ens_order_kernel(const EnsMember *__restrict__ members, const int *__restrict__ 
     }
 }
 
-// field solves of all members: one CTA per member (vlasov_field.cuh)
+// field solves of all members: one thread-block cluster of FC CTAs per member (vlasov_field.cuh)
 __global__ void __launch_bounds__(FS_THREADS) ens_field_kernel(const FieldArgs *__restrict__ fa) {
-    field_solve_body(fa[blockIdx.x]);
+    field_cluster_body(fa[blockIdx.x / FC]);
 }
 
 }  // namespace vl
@@ -385,7 +385,20 @@ int stage(vl_ens *E, int st, cudaStream_t s) {
 
 int field(vl_ens *E, int kind, cudaStream_t s) {
     const int count = (int)E->ctx.size();
-    vl::ens_field_kernel<<<count, vl::FS_THREADS, E->field_smem, s>>>(E->d_field[kind]);
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(vl::FC * count);
+    cfg.blockDim = dim3(vl::FS_THREADS);
+    cfg.dynamicSmemBytes = E->field_smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = vl::FC;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, vl::ens_field_kernel, static_cast<const vl::FieldArgs *>(E->d_field[kind]));
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return efail(VL_ERR_CUDA, std::string("ens_field_kernel: ") + cudaGetErrorString(e));
     return VL_OK;
@@ -468,9 +481,7 @@ int commit(vl_ens *E) {
         // a member launched through its own context: the solve after the Euler stage reads the
         // partials of that context's Euler-stage grid
         if (E->by_order && E->native[i]) E->field[1][i].G = c->stage_grid_g1;
-        const bool staged = vl::field_stage_phase(c->cfg.n, c->cfg.n_modes, c->cfg.nx);
-        for (int k = 0; k < 3; ++k) E->field[k][i].stage_phase = staged ? 1 : 0;
-        E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes, c->cfg.nx, staged));
+        E->field_smem = std::max(E->field_smem, vl::field_solve_smem(c->cfg.n, c->cfg.n_modes));
     }
     std::vector<int> offs;
     std::vector<vl::EnsItem> flat;
@@ -562,7 +573,7 @@ VL_API int vl_ens_create(vl_ctx *const *ctxs, int32_t count, vl_ens **out) {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     cudaFuncSetAttribute(vl::ens_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)vl::FS_DYN_MAX);
+                         (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
     *out = E;
     return VL_OK;
 }

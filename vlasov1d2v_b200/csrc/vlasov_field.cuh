@@ -1,4 +1,5 @@
-// Spectral Poisson solve (main/elliptic.py:117-145) as ONE CTA per problem (sm_100a).
+// Spectral Poisson solve (main/elliptic.py:117-145) as ONE thread-block cluster of FC CTAs per
+// problem (sm_100a).
 //
 // The reference's high-order DFT tensor factors exactly into an element phase and a node
 // transform, T[e, j, m] = exp(-i k_m mid_e) ell[j, m] (main/basis.py:204-228: the phase outer
@@ -6,66 +7,63 @@
 // exp(i k_m x_{e,j}) = exp(i k_m mid_e) q[j, m] with q[j, m] = exp(i k_m (x_{e,j} - mid_e)).  So
 //   c_m    = (dx / L) sum_e ph[e, m] (sum_j rhs[e, j] ell[j, m])              forward
 //   E[e,j] = Re sum_m conj(ph[e, m]) (Ehat_m q[j, m])                           inverse
-// with tables of (nx + 2n) M complex entries instead of 2 nx n M: one CTA of 1024 threads does the
-// whole solve in a few microseconds (the two-launch form spread over ~26 CTAs took ~20 us per
-// solve, launch gaps included).  Steps of one solve:
-//   1. rho = sum over the G moment partials of each node (double-double, fixed order), the
-//      arithmetic node mean (main/timestep.py:155), rhs = kappa (mean - rho)
-//   2. forward: thread (mode m, part) sums its third of the elements; parts folded in order
-//   3. Ehat = -c / (i k), phihat = -c / k^2, the k = 0 mode dropped (CuPy's complex division by
-//      zero + nan_to_num, main/elliptic.py:124-128); C_E[j, m] = Ehat_m q[j, m], C_P likewise
-//   4. inverse: thread (node, part) sums a quarter of the modes; periodic ghost rows of E
-//   5. with FIELD_RECORD: energy (compensated), max |a E|, dt (main/timestep.py:231-242), time,
-//      step counter, history ring, non-finite flag, whether the next step runs
+// with tables of (nx + 2n) M complex entries instead of 2 nx n M.  The FP64 work of one solve
+// (~4e5 multiply-adds at the medium grid) is split over the FC CTAs of a cluster, which exchange
+// the mode coefficients through distributed shared memory; no other launch and no global scratch:
+//   1. every CTA forms the charge from the G moment partials of each node (double-double, fixed
+//      order, so all CTAs hold the same values), the arithmetic node mean (main/timestep.py:155),
+//      rhs = kappa (mean - rho)
+//   2. CTA r: modes [r Mc, (r + 1) Mc): c_m (thread = mode x element range, ranges folded in
+//      order), Ehat = -c / (i k), phihat = -c / k^2, the k = 0 mode dropped (CuPy's complex
+//      division by zero + nan_to_num, main/elliptic.py:124-128); written into every CTA's table
+//   3. cluster barrier; every CTA forms C_E[j, m] = Ehat_m q[j, m] (C_P likewise) for all modes
+//   4. CTA r: nodes [r Nc, (r + 1) Nc): E = Re sum_m conj(ph[e, m]) C_E[j, m] (thread = node x mode
+//      range), periodic ghost rows of E, phi
+//   5. with FIELD_RECORD: energy (compensated) and max |a E| of each CTA's nodes to rank 0 through
+//      distributed shared memory; rank 0 sums them in rank order and does the loop bookkeeping:
+//      dt (main/timestep.py:231-242), time, step counter, history ring, non-finite flag, whether
+//      the next step runs
 #pragma once
+
+#include <cooperative_groups.h>
 
 #include "vlasov_kernels.cuh"
 
 namespace vl {
 
-constexpr int FS_THREADS = 1024;
-constexpr int FS_FWD_PARTS = 3;    // element ranges per mode (M <= 321 -> 963 threads)
-constexpr int FS_INV_PARTS = 4;    // mode ranges per node (256 nodes per pass)
+constexpr int FC = 8;               // CTAs per cluster (portable cluster size)
+constexpr int FS_THREADS = 256;     // threads per CTA
 
-// dynamic shared memory of the solve: C_E and C_P, [n][M] complex each, then (staged) the
-// element phases [nx][M]; the largest dynamic size a launch may ask for (static ~33 KB beside it)
-constexpr size_t FS_DYN_MAX = 190 * 1024;
-__host__ __device__ constexpr size_t field_solve_smem(int n, int M, int nx, bool staged) {
-    return sizeof(double2) * ((size_t)2 * n * M + (staged ? (size_t)nx * M : 0));
-}
-// whether a problem's element phases are staged in shared memory (every grid with nx M small
-// enough: all benchmark grids up to nx = 32)
-__host__ __device__ constexpr bool field_stage_phase(int n, int M, int nx) {
-    return field_solve_smem(n, M, nx, true) <= FS_DYN_MAX;
-}
+// dynamic shared memory of one CTA: C_E and C_P, [n][M] complex each
+__host__ __device__ constexpr size_t field_solve_smem(int n, int M) { return sizeof(double2) * (size_t)2 * n * M; }
 
-__device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
-    __shared__ double s_rho[FIELD_MAX_NODES];                  // rho, then rhs, then E
-    __shared__ double2 s_c[FS_THREADS];                        // forward partial sums, then the inverse fold
-    __shared__ double2 s_E[FIELD_MAX_MODES];
+__device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    __shared__ double s_rhs[FIELD_MAX_NODES];        // rhs, then this CTA's E values
+    __shared__ double2 s_E[FIELD_MAX_MODES];          // Ehat of every mode (filled by every rank)
     __shared__ double2 s_P[FIELD_MAX_MODES];
+    __shared__ double2 s_fold[FS_THREADS];
     __shared__ dd s_red[FS_THREADS / 32];
     __shared__ double s_max[FS_THREADS / 32];
+    __shared__ dd s_rank_energy[FC];                  // rank 0: energy partials of every rank
+    __shared__ double s_rank_max[FC];
+    __shared__ int s_rank_bad[FC];
     extern __shared__ double2 fs_dyn[];
-    static_assert(FS_FWD_PARTS * FIELD_MAX_MODES <= FS_THREADS, "forward thread layout");
-    static_assert(FS_THREADS % FS_INV_PARTS == 0, "inverse thread layout");
-    if (!field_gate(a, true)) return;
     const int tid = threadIdx.x;
     const int n = a.n, nx = a.nx, nn = nx * n, M = a.M;
+    // every CTA of the cluster takes the same decision (the loop state is read before any write
+    // of this launch: rank 0 writes only active and dt, the others read active_next)
+    const bool go = field_gate(a, rank == 0);
+    if (!go) return;   // the whole cluster returns: no barrier is left waiting
     double2 *sCE = fs_dyn;
     double2 *sCP = fs_dyn + (size_t)n * M;
-    // the element phases are read by every thread of the forward and inverse loops: copied once
-    // into shared memory (coalesced, all threads) while the charge is formed, so the loops do not
-    // wait on one global load per mode
-    double2 *sPH = fs_dyn + (size_t)2 * n * M;
-    if (a.stage_phase)
-        for (int q = tid; q < nx * M; q += blockDim.x) sPH[q] = a.phase[q];
-    const double2 *PH = a.stage_phase ? sPH : a.phase;
 
-    // 1. charge
+    // 1. charge (every CTA, identical)
     if (a.charge_in != nullptr) {
-        for (int p = tid; p < nn; p += blockDim.x) s_rho[p] = a.kappa * a.charge_in[p];
-        __syncthreads();   // also publishes the staged phases
+        for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * a.charge_in[p];
+        __syncthreads();
     } else {
         double loc = 0.0, locc = 0.0;
         for (int p = tid; p < nn; p += blockDim.x) {
@@ -74,53 +72,55 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
 #pragma unroll 8
             for (int gg = 0; gg < a.G; ++gg) sacc = dd_add(sacc, dd{a.partials[((size_t)e * a.G + gg) * n + i], 0.0});
             const double rho = sacc.hi + sacc.lo;
-            s_rho[p] = rho;
+            s_rhs[p] = rho;
             const double t = loc + rho;
             locc += (fabs(loc) >= fabs(rho)) ? ((loc - t) + rho) : ((rho - t) + loc);
             loc = t;
         }
         const double mean = block_sum_dd(loc, locc, s_red) / (double)nn;
         __syncthreads();
-        for (int p = tid; p < nn; p += blockDim.x) s_rho[p] = a.kappa * (mean - s_rho[p]);
+        for (int p = tid; p < nn; p += blockDim.x) s_rhs[p] = a.kappa * (mean - s_rhs[p]);
         __syncthreads();
     }
 
-    // 2. forward: c_m = (dx / L) sum_e ph[e, m] sum_j rhs[e, j] ell[j, m]
+    // 2. forward over this rank's modes: thread (mode slot ml, element range part)
+    const int Mc = (M + FC - 1) / FC;
+    const int m0 = rank * Mc;
+    const int parts = FS_THREADS / Mc > 0 ? FS_THREADS / Mc : 1;   // element ranges per mode
     {
-        const int m = tid % FIELD_MAX_MODES, part = tid / FIELD_MAX_MODES;
-        if (part < FS_FWD_PARTS && m < M) {
+        const int ml = tid % Mc, part = tid / Mc;
+        const int m = m0 + ml;
+        double cr = 0.0, ci = 0.0;
+        if (part < parts && m < M) {
             double2 ell[NMAX];
 #pragma unroll
             for (int j = 0; j < NMAX; ++j) ell[j] = (j < n) ? a.ell[(size_t)j * M + m] : make_double2(0.0, 0.0);
-            const int e0 = (part * nx) / FS_FWD_PARTS, e1 = ((part + 1) * nx) / FS_FWD_PARTS;
-            double cr = 0.0, ci = 0.0;
-#pragma unroll 2
+            const int e0 = (part * nx) / parts, e1 = ((part + 1) * nx) / parts;
             for (int e = e0; e < e1; ++e) {
                 double sr = 0.0, si = 0.0;
 #pragma unroll
                 for (int j = 0; j < NMAX; ++j) {
                     if (j < n) {
-                        const double r = s_rho[e * n + j];
+                        const double r = s_rhs[e * n + j];
                         sr = fma(r, ell[j].x, sr);
                         si = fma(r, ell[j].y, si);
                     }
                 }
-                const double2 ph = PH[(size_t)e * M + m];
+                const double2 ph = a.phase[(size_t)e * M + m];
                 cr = fma(ph.x, sr, fma(-ph.y, si, cr));
                 ci = fma(ph.x, si, fma(ph.y, sr, ci));
             }
-            s_c[part * FIELD_MAX_MODES + m] = make_double2(cr, ci);
         }
+        s_fold[tid] = make_double2(cr, ci);
     }
     __syncthreads();
-
-    // 3. Ehat, phihat, and the node-transformed coefficients C[j, m]
-    for (int m = tid; m < M; m += blockDim.x) {
+    for (int ml = tid; ml < Mc; ml += blockDim.x) {
+        const int m = m0 + ml;
+        if (m >= M) break;
         double sr = 0.0, si = 0.0;
-#pragma unroll
-        for (int part = 0; part < FS_FWD_PARTS; ++part) {
-            sr += s_c[part * FIELD_MAX_MODES + m].x;
-            si += s_c[part * FIELD_MAX_MODES + m].y;
+        for (int part = 0; part < parts; ++part) {
+            sr += s_fold[part * Mc + ml].x;
+            si += s_fold[part * Mc + ml].y;
         }
         sr = (sr * a.dx) / a.length;
         si = (si * a.dx) / a.length;
@@ -135,10 +135,14 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
             const double k2 = km * km;
             Ph = make_double2(-(sr / k2), -(si / k2));
         }
-        s_E[m] = Eh;
-        s_P[m] = Ph;
+        for (int r = 0; r < FC; ++r) {   // into every rank's tables
+            cluster.map_shared_rank(s_E, r)[m] = Eh;
+            cluster.map_shared_rank(s_P, r)[m] = Ph;
+        }
     }
-    __syncthreads();
+    cluster.sync();   // every mode's coefficients are in every CTA
+
+    // 3. node-transformed coefficients of every mode
     for (int q = tid; q < n * M; q += blockDim.x) {
         const int j = q / M, m = q - j * M;
         const double2 qq = a.qnode[q];
@@ -148,85 +152,114 @@ __device__ __forceinline__ void field_solve_body(const FieldArgs &a) {
     }
     __syncthreads();
 
-    // 4. inverse: E[e, j] = Re sum_m conj(ph[e, m]) C_E[j, m], phi likewise
+    // 4. inverse over this rank's nodes: thread (node slot, mode range part)
+    const int Nc = (nn + FC - 1) / FC;
+    const int p0 = rank * Nc;
+    const int iparts = FS_THREADS / Nc > 0 ? FS_THREADS / Nc : 1;
+    const int slots = FS_THREADS / iparts;   // node slots per pass
     vl_run_state *st = a.state;
     bool bad = false;
-    for (int p0 = 0; p0 < nn; p0 += FS_THREADS / FS_INV_PARTS) {
-        const int pl = tid % (FS_THREADS / FS_INV_PARTS), part = tid / (FS_THREADS / FS_INV_PARTS);
+    for (int pb = 0; pb < Nc; pb += slots) {
+        const int pl = pb + tid % slots, part = tid / slots;
         const int p = p0 + pl;
         double er = 0.0, pr = 0.0;
-        if (p < nn) {
+        if (part < iparts && pl < Nc && p < nn) {
             const int e = p / n, j = p - e * n;
-            const double2 *ph = PH + (size_t)e * M;
+            const double2 *ph = a.phase + (size_t)e * M;
             const double2 *ce = sCE + (size_t)j * M;
             const double2 *cp = sCP + (size_t)j * M;
+            const int mb = (part * M) / iparts, me = ((part + 1) * M) / iparts;
 #pragma unroll 4
-            for (int m = part; m < M; m += FS_INV_PARTS) {
+            for (int m = mb; m < me; ++m) {
                 const double2 h = ph[m];   // Re(conj(h) c) = h.x c.x + h.y c.y
                 er = fma(h.x, ce[m].x, fma(h.y, ce[m].y, er));
                 pr = fma(h.x, cp[m].x, fma(h.y, cp[m].y, pr));
             }
         }
-        // fold the four parts of each node (lanes pl, pl + 256, ... live in different warps)
         __syncthreads();
-        double2 *fold = s_c;   // the forward sums are no longer needed
-        fold[tid] = make_double2(er, pr);
+        s_fold[tid] = make_double2(er, pr);
         __syncthreads();
-        if (part == 0 && p < nn) {
+        if (part == 0 && pl < Nc && p < nn) {
             double se = 0.0, sp = 0.0;
-#pragma unroll
-            for (int q = 0; q < FS_INV_PARTS; ++q) {
-                se += fold[q * (FS_THREADS / FS_INV_PARTS) + pl].x;
-                sp += fold[q * (FS_THREADS / FS_INV_PARTS) + pl].y;
+            for (int q = 0; q < iparts; ++q) {
+                se += s_fold[q * slots + (tid % slots)].x;
+                sp += s_fold[q * slots + (tid % slots)].y;
             }
             a.E[n + p] = se;
             if (p >= nn - n) a.E[p - (nn - n)] = se;   // E[0] = E[-2]
             if (p < n) a.E[nn + n + p] = se;           // E[-1] = E[1]
             if (a.phi != nullptr) a.phi[p] = sp;
-            s_rho[p] = se;
+            s_rhs[pl] = se;
             bad |= !isfinite(se);
         }
     }
     const int any_bad = __syncthreads_or(bad ? 1 : 0);
-    if (st != nullptr && any_bad && tid == 0) st->status |= 1;
-    if (st == nullptr || !(a.mode & FIELD_RECORD)) return;
+    const bool record = st != nullptr && (a.mode & FIELD_RECORD);
+    if (!record) {
+        if (st != nullptr && any_bad && tid == 0) atomicOr(&st->status, 1);
+        // no CTA may leave while another still writes into its shared memory (step 2 is behind
+        // the barrier above, so nothing remote is pending here)
+        return;
+    }
 
-    // 5. energy, dt and the loop bookkeeping (main/timestep.py:98-103, :184-185, :231-242)
+    // 5. energy and max |a E| of this rank's nodes, to rank 0
     double esq = 0.0, esqc = 0.0, emax = 0.0;
-    for (int q = tid; q < nn; q += blockDim.x) {
-        const double ev = s_rho[q];
-        const double v = a.xw[q % n] * (ev * ev);
+    for (int pl = tid; pl < Nc && p0 + pl < nn; pl += blockDim.x) {
+        const double ev = s_rhs[pl];
+        const double v = a.xw[(p0 + pl) % n] * (ev * ev);
         const double t = esq + v;
         esqc += (fabs(esq) >= fabs(v)) ? ((esq - t) + v) : ((v - t) + esq);
         esq = t;
         emax = fmax(emax, fabs(a.accel * ev));
     }
-    const double energy = 0.5 * block_sum_dd(esq, esqc, s_red);
-    const double maxE = block_max(emax, s_max);
-    if (tid == 0) {
-        const double ab = a.accel * a.bfield;
-        const double s0 = fabs(a.umax);
-        const double s1 = fabs(maxE + fabs(ab * a.vmax));
-        const double s2 = fabs(a.accel * fabs(a.bfield * a.umax));
-        const double dtn = a.courant / (((s0 / a.dx) + (s1 / a.du)) + (s2 / a.dv));
-        const int64_t steps = st->steps + 1;
-        const double time = st->time + dtn;
-        st->dt_next = dtn;
-        st->time = time;
-        st->steps = steps;
-        const int cap = st->hist_capacity;
-        if (cap > 0) {
-            const int slot = (int)((steps - 1) % cap);
-            if (st->energy_hist) st->energy_hist[slot] = energy;
-            if (st->time_hist) st->time_hist[slot] = time;
-            if (st->dt_hist) st->dt_hist[slot] = dtn;
-        }
-        const bool finite = isfinite(energy) && isfinite(dtn) && !any_bad;
-        if (!finite) st->status |= 1;
-        st->active_next = (time < st->final_time) && (steps < st->max_steps) && finite;
+    dd part_e;
+    {
+        dd s = {esq, esqc};
+        for (int off = 16; off > 0; off >>= 1) s = dd_add(s, shfl_down_dd(s, off));
+        if ((tid & 31) == 0) s_red[tid >> 5] = s;
+        __syncthreads();
+        part_e = s_red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) part_e = dd_add(part_e, s_red[w]);
     }
+    const double part_max = block_max(emax, s_max);
+    if (tid == 0) {
+        cluster.map_shared_rank(s_rank_energy, 0)[rank] = part_e;
+        cluster.map_shared_rank(s_rank_max, 0)[rank] = part_max;
+        cluster.map_shared_rank(s_rank_bad, 0)[rank] = any_bad;
+    }
+    cluster.sync();   // rank 0 holds every rank's partials (and no rank exits before it has read)
+    if (rank != 0 || tid != 0) return;
+    dd etot = s_rank_energy[0];
+    double maxE = s_rank_max[0];
+    int bad_any = s_rank_bad[0];
+    for (int r = 1; r < FC; ++r) {
+        etot = dd_add(etot, s_rank_energy[r]);
+        maxE = fmax(maxE, s_rank_max[r]);
+        bad_any |= s_rank_bad[r];
+    }
+    const double energy = 0.5 * (etot.hi + etot.lo);
+    const double ab = a.accel * a.bfield;
+    const double s0 = fabs(a.umax);
+    const double s1 = fabs(maxE + fabs(ab * a.vmax));
+    const double s2 = fabs(a.accel * fabs(a.bfield * a.umax));
+    const double dtn = a.courant / (((s0 / a.dx) + (s1 / a.du)) + (s2 / a.dv));
+    const int64_t steps = st->steps + 1;
+    const double time = st->time + dtn;
+    st->dt_next = dtn;
+    st->time = time;
+    st->steps = steps;
+    const int cap = st->hist_capacity;
+    if (cap > 0) {
+        const int slot = (int)((steps - 1) % cap);
+        if (st->energy_hist) st->energy_hist[slot] = energy;
+        if (st->time_hist) st->time_hist[slot] = time;
+        if (st->dt_hist) st->dt_hist[slot] = dtn;
+    }
+    const bool finite = isfinite(energy) && isfinite(dtn) && !bad_any;
+    if (!finite) st->status |= 1;
+    st->active_next = (time < st->final_time) && (steps < st->max_steps) && finite;
 }
 
-static __global__ void __launch_bounds__(FS_THREADS) field_solve_kernel(const FieldArgs a) { field_solve_body(a); }
+static __global__ void __launch_bounds__(FS_THREADS) field_solve_kernel(const FieldArgs a) { field_cluster_body(a); }
 
 }  // namespace vl

@@ -227,7 +227,6 @@ struct FieldArgs {
     const double2 *ell;       // [n][M]   T[e, j, m] = phase[e, m] ell[j, m]
     const double2 *phase;     // [nx][M]  exp(-i k_m mid_e)
     const double2 *qnode;     // [n][M]   exp(i k_m x_{e,j}) = conj(phase[e, m]) qnode[j, m]
-    int stage_phase;          // 1: the solve copies phase into shared memory first (when it fits)
     const double *k;          // [M]
     const double *xw;         // [n]
     int nx, n, M;
