@@ -1,13 +1,14 @@
 // FP32 fused SSP-RK stage kernel for n = 8 (sm_100a): packed-FP32 contractions.
 //
 // Same tile, shared-memory stage and TMA pipeline as the fragment kernel (vlasov_stage_frag.cuh,
-// FragGeom<float>): tile = (x element e, u element a, 4 consecutive v elements), warp w = v element
-// of the tile, lane = 4 g + t owns x node i = g and the column pair k = 2t, 2t + 1 for all eight j.
+// FragGeom<float>): tile = (x element e, u element a, 4 consecutive v elements); warp w holds x
+// nodes 2w and 2w + 1 of all four elements, lane = 16 h + 4 b + t owns x node g = 2w + h of element b
+// and the column pair k = 2t, 2t + 1 for all eight j (a warp store covers two whole tile rows).
 // Every product of a coefficient with the thread's two columns is one packed FMA
 // (fma.rn.f32x2: two FP32 lanes per instruction), which halves the issue slots of the three
 // contractions, the lifts, the flux products, the RK combination and the moment:
 //   x:  {d, d'} = sum_m {up[g][m], up[g][m]} * F[m][j][k, k+1]   8 pair loads (broadcast across
-//                                                                 the eight lanes of one t)
+//                                                                 the two x nodes of a warp)
 //   v:  d_k = sum_q {up[k][2q], up[k][2q+1]} * F[g][j][2q, 2q+1]  the element's k-line as two
 //                                                                 16-byte loads, pairs over m
 //   u:  {d, d'} = sum_m {up[j][m], up[j][m]} * F[g][m][k, k+1]   j compile-time: the coefficient
@@ -57,21 +58,25 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
     using G = FragGeom<float>;
     constexpr int N = G::N, P = G::P, W = G::W, PS = G::PS, WF = G::WF, PSF = G::PSF;
     constexpr int COLS = G::COLS, EPT = G::EPT;
-    static_assert(G::JS == 1, "one warp per v element");
+    static_assert(G::THREADS == 128 && EPT == 4, "four warps of two x nodes each");
     if (a.state != nullptr && a.state->active == 0) return;
 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~(uintptr_t)127);
     __shared__ __align__(8) uint64_t full[2];
-    __shared__ dd sRed[EPT][N];
+    __shared__ dd sRed[N];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int w = tid >> 5;          // v element of the tile
-    const int g = lane >> 2;         // x node i of the thread's outputs
-    const int t = lane & 3;          // columns 2t, 2t + 1 of the element
-    const int wc = w * N;            // first tile column of the element
+    // warp w covers x nodes 2w, 2w + 1 of all four v elements of the tile: lane = 16 h + 4 b + t
+    // owns x node g = 2w + h, element b and its columns 2t, 2t + 1, so one warp store writes two
+    // whole 128-byte rows of the output tile
+    const int w = tid >> 5;
+    const int g = 2 * w + (lane >> 4);   // x node i of the thread's outputs
+    const int b = (lane >> 2) & 3;       // v element of the tile
+    const int t = lane & 3;              // columns 2t, 2t + 1 of the element
+    const int wc = b * N;                // first tile column of the element
     const int cl = wc + 2 * t;       // first tile column of the thread
     const int k0 = 2 * t, k1 = 2 * t + 1;
 
@@ -164,6 +169,19 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
     float *gout = static_cast<float *>(a.ghost_out);
     const bool ghost = gout != nullptr && (e == 0 || e == nx - 1);
     double mk0 = 0.0, mk1 = 0.0;   // sum over rows of (w_j / J_u) out[.., j, k] for the two columns
+    // v-node coordinates of the thread's columns, loaded one tile ahead of their use
+    auto vnodes = [&](int q, double &x0, double &x1) {
+        x0 = x1 = 0.0;
+        if (q >= ntile_cta) return;
+        const int tq = blockIdx.x + q * gridDim.x;
+        const int bq = (tq - (tq / nbt) * nbt) * EPT;
+        if (b < min(EPT, nv - bq)) {
+            x0 = a.v_nodes[(bq + 1) * N + cl];
+            x1 = a.v_nodes[(bq + 1) * N + cl + 1];
+        }
+    };
+    double vn0, vn1;
+    vnodes(0, vn0, vn1);
 
     for (int q = 0; q < ntile_cta; ++q) {
         const int s = q & 1;
@@ -172,9 +190,10 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
         const int b0 = (tt - au * nbt) * EPT;
         const int nb = min(EPT, nv - b0);
         const int Ag = au + 1;
-        const bool act = w < nb;
+        const bool act = b < nb;
         const int col = (b0 + 1) * N + cl;   // global v-node column of the first output
-        const double vc0 = act ? a.v_nodes[col] : 0.0, vc1 = act ? a.v_nodes[col + 1] : 0.0;
+        const double vc0 = vn0, vc1 = vn1;
+        vnodes(q + 1, vn0, vn1);
         if (!mbar_wait_bounded(&full[s], (uint32_t)((q >> 1) & 1))) {
             if (a.err != nullptr) atomicOr(a.err, 2);
             return;
@@ -303,18 +322,15 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
     }
 
     if (a.partials == nullptr) return;
-    // moment partial of x node g: sum over the thread's columns, the quad, the warps
+    // moment partial of x node g: sum over the thread's columns, then over the 16 lanes of the
+    // half-warp that holds node g (its four elements and column pairs)
     dd v = two_sum(tb.wv[k0] * mk0, tb.wv[k1] * mk1);
-    v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 1), __shfl_xor_sync(0xffffffffu, v.lo, 1)});
-    v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, 2), __shfl_xor_sync(0xffffffffu, v.lo, 2)});
-    if (t == 0) sRed[w][g] = v;
-    __syncthreads();
-    if (tid < N) {
-        dd sum = sRed[0][tid];
 #pragma unroll
-        for (int ww = 1; ww < EPT; ++ww) sum = dd_add(sum, sRed[ww][tid]);
-        a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * N + tid] = sum.hi + sum.lo;
-    }
+    for (int off = 1; off < 16; off <<= 1)
+        v = dd_add(v, dd{__shfl_xor_sync(0xffffffffu, v.hi, off), __shfl_xor_sync(0xffffffffu, v.lo, off)});
+    if ((lane & 15) == 0) sRed[g] = v;
+    __syncthreads();
+    if (tid < N) a.partials[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * N + tid] = sRed[tid].hi + sRed[tid].lo;
 }
 
 }  // namespace vl
