@@ -236,6 +236,74 @@ int gen_bg_map(vl_ctx *c, const float *ptr, CUtensorMap *out) {
     return VL_OK;
 }
 
+// 4-D view (2R, U n / 2, n, X) of an FP32 state for the generic kernel's paired-row form (R =
+// (nv+2) n floats per row, two rows per 16-byte-multiple pair): which 0 = tile (WB, NPJ, n, 1),
+// 1 = x-node plane (WB, NPJ, 1, 1), 2 = one row of every x node (WB, 1, n, 1)
+template <int N, typename T>
+int gen_pair_map(vl_ctx *c, const void *ptr, int which, CUtensorMap *out) {
+    using G = vl::GenPairGeom<N, T>;
+    auto key = std::make_pair(ptr, 40 + which);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2, X = c->cfg.nx + 2, es = sizeof(T);
+    const cuuint64_t R = V * N;
+    cuuint64_t dims[4] = {2 * R, U * N / 2, (cuuint64_t)N, X};
+    cuuint64_t strides[3] = {2 * R * es, U * N * R * es, U * N * R * N * es};
+    cuuint32_t box[4] = {(cuuint32_t)G::WB, 1, 1, 1};
+    if (which == 0) {
+        box[1] = G::NPJ;
+        box[2] = N;
+    } else if (which == 1) {
+        box[1] = G::NPJ;
+    } else {
+        box[2] = N;
+    }
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (paired rows) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
+// 2-D view (2R, U n / 2) of a background-split table for the paired-row form, box (WB, NPJ)
+template <int N, typename T>
+int gen_pair_bg_map(vl_ctx *c, const float *ptr, CUtensorMap *out) {
+    using G = vl::GenPairGeom<N, T>;
+    auto key = std::make_pair(static_cast<const void *>(ptr), 50);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2;
+    const cuuint64_t R = V * N;
+    cuuint64_t dims[2] = {2 * R, U * N / 2};
+    cuuint64_t strides[1] = {2 * R * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)G::WB, (cuuint32_t)G::NPJ};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (paired rows, background) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
 // coefficient tables of the FP32 n = 8 kernel (pairs for the packed FMAs), built once per context
 const vl::F32Tables &f32_tables(vl_ctx *c) {
     if (!c->f32_tables_ready) {
@@ -343,6 +411,29 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             }
         }
     }
+    if constexpr (sizeof(T) == 4) {
+        if (c->stage_kernel == VL_STAGE_GEN && c->gen_pair) {
+            using G = vl::GenPairGeom<N, T>;
+            if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
+                 reinterpret_cast<uintptr_t>(a.fn) | reinterpret_cast<uintptr_t>(a.ghost_out) |
+                 reinterpret_cast<uintptr_t>(a.bg_rb) | reinterpret_cast<uintptr_t>(a.bg_eu)) % 16)
+                return fail(VL_ERR_INVALID, "state buffers must be 16-byte aligned");
+            vl::GenMaps maps;
+            std::memset(&maps, 0, sizeof(maps));
+            int rc;
+            if ((rc = gen_pair_map<N, T>(c, a.in, 0, &maps.in_tile))) return rc;
+            if ((rc = gen_pair_map<N, T>(c, a.fn ? a.fn : a.in, 0, &maps.fn_tile))) return rc;
+            if ((rc = gen_pair_map<N, T>(c, a.in, 1, &maps.xface))) return rc;
+            if ((rc = gen_pair_map<N, T>(c, a.in, 2, &maps.uface))) return rc;
+            if (a.bg_rb != nullptr) {
+                if ((rc = gen_pair_bg_map<N, T>(c, a.bg_eu, &maps.bg_eu))) return rc;
+                if ((rc = gen_pair_bg_map<N, T>(c, a.bg_rb, &maps.bg_rb))) return rc;
+            }
+            return check_launch(launch(c, vl::stage_gen_pair_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(),
+                                       s, a, tb, maps),
+                                "stage_gen_pair_kernel");
+        }
+    }
     if (c->stage_kernel == VL_STAGE_GEN && c->gen_tma) {
         using G = vl::GenTmaGeom<N, T>;
         if ((reinterpret_cast<uintptr_t>(a.in) | reinterpret_cast<uintptr_t>(a.out) |
@@ -416,8 +507,20 @@ int stage(vl_ctx *c, const vl::StageArgs &a, cudaStream_t s) {
 }
 
 template <int N, typename T>
-int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma) {
+int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool gpair) {
     int blocks = 0;
+    if constexpr (sizeof(T) == 4) {
+        if (gen && gpair) {
+            using G = vl::GenPairGeom<N, T>;
+            const size_t smem = G::smem_bytes();
+            cudaFuncSetAttribute(vl::stage_gen_pair_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_pair_kernel<N, T>, G::THREADS,
+                                                              smem) != cudaSuccess)
+                return 1;
+            return blocks > 0 ? blocks : 1;
+        }
+    }
     if (gen && gtma) {
         using G = vl::GenTmaGeom<N, T>;
         const size_t smem = G::smem_bytes();
@@ -511,18 +614,18 @@ bool tma_supported_t(const vl_config &g) {
 }
 
 template <typename T>
-int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma) {
+int stage_occupancy(int n, bool tma, bool frag, bool gen, bool gtma, bool gpair) {
     switch (n) {
-        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma);
-        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma);
-        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma);
-        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma);
-        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma);
-        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma);
-        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma);
-        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma);
-        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma);
-        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma);
+        case 1: return stage_occupancy_t<1, T>(tma, frag, gen, gtma, gpair);
+        case 2: return stage_occupancy_t<2, T>(tma, frag, gen, gtma, gpair);
+        case 3: return stage_occupancy_t<3, T>(tma, frag, gen, gtma, gpair);
+        case 4: return stage_occupancy_t<4, T>(tma, frag, gen, gtma, gpair);
+        case 5: return stage_occupancy_t<5, T>(tma, frag, gen, gtma, gpair);
+        case 6: return stage_occupancy_t<6, T>(tma, frag, gen, gtma, gpair);
+        case 7: return stage_occupancy_t<7, T>(tma, frag, gen, gtma, gpair);
+        case 8: return stage_occupancy_t<8, T>(tma, frag, gen, gtma, gpair);
+        case 9: return stage_occupancy_t<9, T>(tma, frag, gen, gtma, gpair);
+        case 10: return stage_occupancy_t<10, T>(tma, frag, gen, gtma, gpair);
         default: return 1;
     }
 }
@@ -853,10 +956,13 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     }();
     const bool gen_tma32 = cfg->precision == VL_FP32 && ((size_t)(cfg->nv + 2) * n) % 4 == 0 && !no_gen_tma &&
                            encode_fn() != nullptr;
+    // FP32 rows of R = 2 mod 4 floats over an even number of rows: the paired-row TMA form
+    const bool gen_pair32 = cfg->precision == VL_FP32 && ((size_t)(cfg->nv + 2) * n) % 4 == 2 &&
+                            ((size_t)(cfg->nu + 2) * n) % 2 == 0 && !no_gen_tma && encode_fn() != nullptr;
     c->stage_kernel = c->use_frag                                  ? VL_STAGE_FRAG
                       : cfg->precision == VL_FP64                  ? VL_STAGE_GEN
                       : c->use_tma                                 ? VL_STAGE_TMA
-                      : gen_tma32                                  ? VL_STAGE_GEN
+                      : (gen_tma32 || gen_pair32)                  ? VL_STAGE_GEN
                                                                    : VL_STAGE_PENCIL;
     {
         const char *env = getenv("VLASOV1D2V_STAGE_KERNEL");
@@ -873,9 +979,10 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
     // generic kernel in its TMA form: FP64 rows of a 16-byte multiple (V n even), FP32 as above
     c->gen_tma = gen && (cfg->precision == VL_FP64 ? ((size_t)(cfg->nv + 2) * n) % 2 == 0 : gen_tma32) &&
                  encode_fn() != nullptr && !no_gen_tma;
+    c->gen_pair = gen && !c->gen_tma && gen_pair32;
     const int occ = cfg->precision == VL_FP64
-                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma)
-                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma);
+                        ? stage_occupancy<double>(n, c->use_tma, c->use_frag, gen, c->gen_tma, false)
+                        : stage_occupancy<float>(n, c->use_tma, c->use_frag, gen, c->gen_tma, c->gen_pair);
     const int bt = stage_epw(c);
     const int tiles = cfg->nu * ((cfg->nv + bt - 1) / bt);
     // one wave: at most occ x SMs resident CTAs in total (a second partial wave would double

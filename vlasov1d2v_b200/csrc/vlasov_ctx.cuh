@@ -42,6 +42,7 @@ struct vl_ctx {
     bool use_frag = false;        // n = 8: quad-fragment stage kernel (tensor cores in FP64)
     int stage_kernel = VL_STAGE_GEN;   // which stage kernel the launches use (vl_stage_kernel)
     bool gen_tma = false;         // generic stage kernel in its TMA form (FP64, aligned rows)
+    bool gen_pair = false;        // generic stage kernel in its paired-row TMA form (FP32, R = 2 mod 4)
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
     const float *bg_eu = nullptr;
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer

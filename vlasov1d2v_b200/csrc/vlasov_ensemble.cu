@@ -704,7 +704,7 @@ VL_API int vl_ens_schedule_by_order(vl_ens *E, int32_t items_per_cta, uint32_t n
         const vl_ctx *c = E->ctx[i];
         if (native_orders == VL_ENS_NATIVE_AUTO)
             native[i] = c->stage_kernel == VL_STAGE_FRAG || c->stage_kernel == VL_STAGE_TMA ||
-                        (c->stage_kernel == VL_STAGE_GEN && c->gen_tma);
+                        (c->stage_kernel == VL_STAGE_GEN && (c->gen_tma || c->gen_pair));
         else
             native[i] = (native_orders >> c->cfg.n) & 1u;
     }

@@ -35,6 +35,11 @@
 // (off < 16 bytes per tile), and the column pairs are read as two scalar loads.  Every box lands
 // on a 128-byte-aligned shared-memory address.
 //
+// Paired-row TMA form (stage_gen_pair_kernel; FP32 rows of R = 2 mod 4 floats, e.g. the large
+// configuration's 66 x 9): two rows are a 16-byte multiple, so each array is loaded as a box of its
+// even rows and a box of its odd rows (GenPairGeom); the tile body is instantiated for both
+// parities of the tile's first row, so every row offset stays a compile-time constant.
+//
 #pragma once
 
 #include <cuda_runtime.h>
@@ -156,6 +161,8 @@ struct GenGeom {
 };
 
 // tensor maps of the TMA form (5-D views of the state: v node, j, a, i, e)
+// (paired-row form: 4-D views (2R, U n / 2, n, X) with boxes (WB, NPJ, n, 1), (WB, NPJ, 1, 1) and
+// (WB, 1, n, 1); background tables 2-D (2R, U n / 2) with box (WB, NPJ))
 struct GenMaps {
     CUtensorMap in_tile;   // box (WB, RJ, 1, n, 1) over the stage input
     CUtensorMap fn_tile;   // the same box over f^n
@@ -209,8 +216,52 @@ struct GenTmaGeom {
     static_assert(WB <= 256, "TMA box width");
 };
 
+// Paired-row TMA form (FP32 rows of R = (nv+2) n floats with R = 2 mod 4, an even number U n of
+// rows): a row is not a 16-byte multiple but two consecutive rows are, so the state is viewed as
+// 4-D (2R floats of a row pair, U n / 2 pairs, n x nodes, x elements) and every array of a tile
+// is loaded as two boxes: the even rows (pair columns [0, R)) and the odd rows ([R, 2R)), each box
+// starting at the 16-byte boundary at or below its rows' left v trace.  The odd rows then sit
+// 2 floats off the even ones; each parity has its own column offset in shared memory.
+template <int N, typename T, int EPT_ = GenEpt<N, T>::value>
+struct GenPairGeom {
+    using GT = GenTmaGeom<N, T, EPT_>;
+    static constexpr int EPT = EPT_;
+    static constexpr int Q = GT::Q;
+    static constexpr int WB = GT::WB;                  // box width: tile + traces at any offset
+    static constexpr int NPJ = (N + 2) / 2;            // row pairs spanning the n rows of a u element
+    static constexpr int PS = NPJ * WB;                // plane stride within one parity
+    static constexpr int THREADS = GT::THREADS;
+    static constexpr int NST = 2;
+    static constexpr size_t al(size_t b) { return (b + 127) & ~(size_t)127; }
+    static constexpr size_t BLK = al(sizeof(T) * (size_t)N * PS);       // one parity of the tile
+    static constexpr size_t IN_B = 2 * BLK;
+    static constexpr size_t FN_B = IN_B;
+    static constexpr size_t FPB = al(sizeof(T) * (size_t)PS);          // one parity of a plane / table
+    static constexpr size_t XF_B = 4 * FPB;                            // [side][parity]
+    static constexpr size_t FSIDE_B = al(sizeof(T) * (size_t)N * WB);  // one u-trace side [i][WB]
+    static constexpr size_t UF_B = 2 * FSIDE_B;
+    static constexpr size_t BG_B = sizeof(T) == 4 ? 4 * FPB : 0;       // [table][parity]
+    static constexpr size_t UX_B = GT::UX_B;
+    static constexpr size_t STAGE_B = IN_B + FN_B + XF_B + UF_B + BG_B + UX_B;
+    static constexpr uint32_t TX_IN = sizeof(T) * WB * NPJ * N;        // one parity
+    static constexpr uint32_t TX_XF = sizeof(T) * WB * NPJ;            // one side, one parity
+    static constexpr uint32_t TX_UF = sizeof(T) * WB * N;              // one side
+    static constexpr uint32_t TX_BG = sizeof(float) * WB * NPJ;        // one table, one parity
+    static constexpr uint32_t TX_UX = GT::TX_UX;
+    static constexpr size_t smem_bytes() {
+        const size_t s = NST * STAGE_B;
+        const size_t red = sizeof(dd) * (size_t)THREADS;
+        return (s > red ? s : red) + 128;
+    }
+    static constexpr int SMEM_CTAS = (int)((227 * 1024) / (smem_bytes() + 1024));
+    static constexpr int REG_CTAS = GT::REG_CTAS;
+    static constexpr int MINB_ = SMEM_CTAS < REG_CTAS ? SMEM_CTAS : REG_CTAS;
+    static constexpr int MINB = MINB_ < 1 ? 1 : (MINB_ > 4 ? 4 : MINB_);
+    static_assert(WB <= 256, "TMA box width");
+};
+
 // shared-memory layout constants of the three forms (row lengths, plane strides, array bytes):
-// MODE 0 slot rows (cp.async), 1 TMA rows
+// MODE 0 slot rows (cp.async), 1 TMA rows, 2 paired TMA rows
 template <int MODE, int N, typename T, int EPT>
 struct GenLayout {
     using GG = GenGeom<N, T, EPT>;
@@ -229,6 +280,17 @@ struct GenLayout<1, N, T, EPT> {
     static constexpr size_t S_IN = GT::IN_B, S_FN = GT::FN_B, S_XF = GT::XF_B, S_UF = GT::UF_B;
     static constexpr size_t S_BG = GT::BG_B, S_STAGE = GT::STAGE_B;
 };
+template <int N, typename T, int EPT>
+struct GenLayout<2, N, T, EPT> {
+    using GP = GenPairGeom<N, T, EPT>;
+    static constexpr int RIN = GP::WB, PIN = GP::PS, RFN = GP::WB, PFN = GP::PS, RFC = GP::WB, Q = GP::Q;
+    static constexpr int FS = (int)(GP::FSIDE_B / sizeof(T));   // second u-trace side (elements)
+    static constexpr int BLK = (int)(GP::BLK / sizeof(T));      // odd-row block of IN / FN (elements)
+    static constexpr int FPB = (int)(GP::FPB / sizeof(T));      // one parity of a face plane / table
+    static constexpr int BGS = (int)(2 * GP::FPB / sizeof(float));   // second background table (floats)
+    static constexpr size_t S_IN = GP::IN_B, S_FN = GP::FN_B, S_XF = GP::XF_B, S_UF = GP::UF_B;
+    static constexpr size_t S_BG = GP::BG_B, S_STAGE = GP::STAGE_B;
+};
 
 template <typename T>
 struct GenPair;
@@ -245,10 +307,11 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB, bool TMA = false>
+template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PAIR = false>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
                                                int g, int G, unsigned char *smem,
                                                const GenMaps *maps = nullptr) {
+    static_assert(!PAIR || (TMA && sizeof(T) == 4), "the paired-row form is a TMA form of FP32 states");
     constexpr bool CONTIG = TMA;   // contiguous rows (scalar pair loads)
     constexpr bool MB = TMA;       // stages filled by asynchronous bulk copies on mbarriers
     using GG = GenGeom<N, T, EPT>;
@@ -256,7 +319,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     constexpr int P = GG::P, SL = GG::SL, H = GG::H, LH = GG::LH, W = GG::W, WN = GG::WN, WF = GG::WF;
     constexpr int PS = GG::PS, PSF = GG::PSF, NST = GG::NST, NW = GG::NW, NT = GG::THREADS;
     // shared-memory geometry of the form in use (TMA: contiguous rows of the state)
-    using L = GenLayout<TMA ? 1 : 0, N, T, EPT>;
+    using L = GenLayout<PAIR ? 2 : (TMA ? 1 : 0), N, T, EPT>;
     constexpr int RIN = L::RIN;      // IN row length
     constexpr int PIN = L::PIN;      // IN plane stride
     constexpr int RFN = L::RFN;      // FN row length
@@ -394,7 +457,40 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     };
     // TMA form: one thread loads the tile's boxes into stage s
     auto issue_tma = [&](int s, int tt) {
-        if constexpr (TMA) {
+        if constexpr (PAIR) {
+            // paired rows: even rows at pair columns [0, R), odd rows at [R, 2R); each box starts at
+            // the 16-byte boundary at or below its rows' left v trace
+            using GP = GenPairGeom<N, T, EPT>;
+            const int au = tt / nbt;
+            const int b0 = (tt - au * nbt) * EPT;
+            const int Ag = au + 1;
+            const int R = (nv + 2) * N;
+            const int cL = (b0 + 1) * N - 1;
+            const int xs0 = cL & ~(GP::Q - 1), xs1 = (R + cL) & ~(GP::Q - 1);
+            const int r0 = Ag * N, p0 = r0 >> 1;
+            unsigned char *st = stage_ptr(s);
+            unsigned char *xf = st + S_IN + S_FN;
+            unsigned char *uf = xf + S_XF;
+            const uint32_t tx = 2 * GP::TX_IN * (with_fn ? 2 : 1) + 4 * GP::TX_XF + 2 * GP::TX_UF + GP::TX_UX +
+                                (with_bg ? 4 * GP::TX_BG : 0);
+            mbar_arrive_expect_tx(&gfull[s], tx);
+#pragma unroll
+            for (int par = 0; par < 2; ++par) {
+                const int xs = par ? xs1 : xs0;
+                tma_load_4d(st + par * GP::BLK, &maps->in_tile, &gfull[s], xs, p0, 0, Eg);
+                if (with_fn) tma_load_4d(st + S_IN + par * GP::BLK, &maps->fn_tile, &gfull[s], xs, p0, 0, Eg);
+                tma_load_4d(xf + par * GP::FPB, &maps->xface, &gfull[s], xs, p0, N - 1, El);
+                tma_load_4d(xf + (2 + par) * GP::FPB, &maps->xface, &gfull[s], xs, p0, 0, Er);
+                if (with_bg) {
+                    tma_load_2d(uf + S_UF + par * GP::FPB, &maps->bg_eu, &gfull[s], xs, p0);
+                    tma_load_2d(uf + S_UF + (2 + par) * GP::FPB, &maps->bg_rb, &gfull[s], xs, p0);
+                }
+            }
+            const int rl = r0 - 1, rr = r0 + N;   // u traces: row n-1 of element a-1, row 0 of a+1
+            tma_load_4d(uf, &maps->uface, &gfull[s], (rl & 1) ? xs1 : xs0, rl >> 1, 0, Eg);
+            tma_load_4d(uf + GP::FSIDE_B, &maps->uface, &gfull[s], (rr & 1) ? xs1 : xs0, rr >> 1, 0, Eg);
+            bulk_load(uf + S_UF + S_BG, a.u_nodes + ((Ag * N) & ~1), GP::TX_UX, &gfull[s]);
+        } else if constexpr (TMA) {
             using GT = GenTmaGeom<N, T, EPT>;
             const int au = tt / nbt;
             const int b0 = (tt - au * nbt) * EPT;
@@ -489,6 +585,13 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         const int ebase = TMA ? (cL - (cL & ~(L::Q - 1))) + 1 + b * N : H + b * SL;
         const int cin = ebase + 2 * p;
         const int cfc = CONTIG ? cin : cs;
+        // paired rows: column of element b's node 0 in the even and in the odd rows
+        const int Rrow = (nv + 2) * N;
+        const int e0 = (cL & (L::Q - 1)) + 1 + b * N;
+        const int e1 = ((Rrow + cL) & (L::Q - 1)) + 1 + b * N;
+        (void)Rrow;
+        (void)e0;
+        (void)e1;
         const double *sUX = sUX0 + (MB ? ((Ag * N) & 1) : 0);
         auto ld2 = [&](const T *q2) -> V2 {
             if constexpr (CONTIG) {
@@ -500,19 +603,47 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 return *reinterpret_cast<const V2 *>(q2);
             }
         };
-        if (act) {
+        // the tile body, for the parity RP of the tile's first row among the U n rows (paired form;
+        // 0 otherwise): row r of the tile is row (RP + r) / 2 of parity (RP + r) % 2
+        auto tile_rows = [&](auto rpc) {
+            constexpr int RP = decltype(rpc)::value;
+            (void)RP;
+            // IN / FN layout: pointer to node 0 of element b in row r of plane pl
+            auto rowp = [&](const T *arr, int pl, int r) -> const T * {
+                if constexpr (PAIR) {
+                    const int par = (RP + r) & 1, idx = (RP + r) >> 1;
+                    return arr + par * L::BLK + pl * PIN + idx * RIN + (par ? e1 : e0);
+                } else {
+                    return arr + pl * PIN + r * RIN + ebase;
+                }
+            };
+            // face / background layout ([side][parity][pair][WB] in the paired form): node 0 of
+            // element b in row r of side sd
+            auto facep = [&](const T *arr, int sd, int r) -> const T * {
+                if constexpr (PAIR) {
+                    const int par = (RP + r) & 1, idx = (RP + r) >> 1;
+                    return arr + (2 * sd + par) * L::FPB + idx * RFC + (par ? e1 : e0);
+                } else {
+                    return arr + sd * FS + r * RFC + cfc - 2 * p;
+                }
+            };
             const double sd0 = accel * (Ei + bfield * vn0);
             const double sd1 = accel * (Ei + bfield * vn1);
             const T sp0 = (T)sd0, sp1 = (T)sd1;
             V2 fu[N];
 #pragma unroll
-            for (int m = 0; m < N; ++m) fu[m] = ld2(sIn + i * PIN + m * RIN + cin);
-            const V2 ufl = ld2(sUF + i * RFC + cfc);
-            const V2 ufr = ld2(sUF + FS + i * RFC + cfc);
+            for (int m = 0; m < N; ++m) fu[m] = ld2(rowp(sIn, i, m) + 2 * p);
+            V2 ufl, ufr;
+            if constexpr (PAIR) {   // row n-1 of element a-1: parity RP + 1; row 0 of a+1: RP + n
+                ufl = ld2(sUF + i * RFC + (((RP + 1) & 1) ? e1 : e0) + 2 * p);
+                ufr = ld2(sUF + FS + i * RFC + (((RP + N) & 1) ? e1 : e0) + 2 * p);
+            } else {
+                ufl = ld2(sUF + i * RFC + cfc);
+                ufr = ld2(sUF + FS + i * RFC + cfc);
+            }
             const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
             const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
             T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
-            const T *prow = sIn + i * PIN + ebase;   // k-line of element b at j = 0
 #pragma unroll
             for (int j = 0; j < N; ++j) {
                 const double uxd = sUX[j];
@@ -520,7 +651,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 const bool xpos = uxd >= 0.0;
                 const bool vpos = svd >= 0.0;
                 // x: sum_m up[i][m] F[m][j][k] + lifts
-                const T *pc = sIn + j * RIN + cin;
+                const T *pc = rowp(sIn, 0, j) + 2 * p;
                 T dx0 = (T)0, dx1 = (T)0;
                 V2 cm0, cmL;
 #pragma unroll
@@ -531,8 +662,8 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     dx0 = fma(upi[m], cv.x, dx0);
                     dx1 = fma(upi[m], cv.y, dx1);
                 }
-                const V2 xf0 = ld2(sXF + j * RFC + cfc);
-                const V2 xf1 = ld2(sXF + FS + j * RFC + cfc);
+                const V2 xf0 = ld2(facep(sXF, 0, j) + 2 * p);
+                const V2 xf1 = ld2(facep(sXF, 1, j) + 2 * p);
                 const V2 xl = xpos ? xf0 : cm0;
                 const V2 xr = xpos ? cmL : xf1;
                 dx0 = fma(xig0, xl.x, dx0);
@@ -540,7 +671,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 dx1 = fma(xig0, xl.y, dx1);
                 dx1 = fma(-xig1, xr.y, dx1);
                 // v: sum_m F[i][j][m] up[k][m] + lifts (the element's k-line)
-                const T *pa = prow + j * RIN;
+                const T *pa = rowp(sIn, i, j);   // k-line of element b
                 T line[2 * P];
 #pragma unroll
                 for (int m2 = 0; m2 < P; ++m2) {
@@ -576,7 +707,13 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
                 if (with_bg) {   // RHS of the x-independent background
                     float2 eu, rb;
-                    const float *pbg = sBG + j * RFC + cfc;
+                    const float *pbg;
+                    if constexpr (PAIR) {   // [table][parity][pair][WB]
+                        const int par = (RP + j) & 1, idx = (RP + j) >> 1;
+                        pbg = sBG + par * L::FPB + idx * RFC + (par ? e1 : e0) + 2 * p;
+                    } else {
+                        pbg = sBG + j * RFC + cfc;
+                    }
                     if constexpr (CONTIG) {
                         eu = make_float2(pbg[0], pbg[1]);
                         rb = make_float2(pbg[L::BGS], pbg[L::BGS + 1]);
@@ -596,7 +733,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     o.x = fma(dtT, r0, fij.x);
                     o.y = fma(dtT, r1, fij.y);
                 } else {
-                    const V2 fnv = ld2(sFn + i * PFN + j * RFN + cfc);
+                    const V2 fnv = PAIR ? ld2(rowp(sFn, i, j) + 2 * p) : ld2(sFn + i * PFN + j * RFN + cfc);
                     o.x = rk_combine(c0, c1, c2dt, fnv.x, fij.x, r0);
                     o.y = rk_combine(c0, c1, c2dt, fnv.y, fij.y, r1);
                 }
@@ -621,6 +758,16 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 }
                 mk0 = fma(tb.wu[j], (double)o.x, mk0);
                 mk1 = fma(tb.wu[j], (double)o.y, mk1);
+            }
+        };
+        if (act) {
+            if constexpr (PAIR) {
+                if ((Ag * N) & 1)
+                    tile_rows(std::integral_constant<int, 1>{});
+                else
+                    tile_rows(std::integral_constant<int, 0>{});
+            } else {
+                tile_rows(std::integral_constant<int, 0>{});
             }
         }
         __syncthreads();   // stage q % NST consumed before it is refilled
@@ -665,6 +812,19 @@ stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> t
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
     gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true>(
+        a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
+}
+
+// paired-row TMA form (FP32 rows of R = 2 mod 4 floats)
+template <int N, typename T>
+__global__ void __launch_bounds__(GenPairGeom<N, T>::THREADS, GenPairGeom<N, T>::MINB)
+stage_gen_pair_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
+                      const __grid_constant__ GenMaps maps) {
+    if (a.state != nullptr && a.state->active == 0) return;
+    extern __shared__ __align__(16) unsigned char gen_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
+    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true, true>(
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
 }
 
