@@ -91,7 +91,7 @@ def kernel_only(args):
         ctx.rk_stage(0, f, None, sa, E, dt, partials=ctx.workspace)
         ctx.rk_stage(1, sa, f, sb, E, dt, partials=ctx.workspace)
         ctx.rk_stage(2, sb, f, sa, E, dt, partials=ctx.workspace)
-        # the standalone moment and the single-CTA field solve of the same problem
+        # the standalone moment and the cluster field solve of the same problem
         ctx.moment(f, rho)
         ctx.poisson((rho.mean() - rho).contiguous(), E, phi)
     torch.cuda.synchronize()
@@ -328,23 +328,28 @@ def measure_precision(precision, steps, warmup, reps, dist, res=None, order=None
     if stt.status != 0:
         raise RuntimeError("non-finite state during the benchmark")
 
-    # per-kernel timing of the three stage kinds (the dominant kernel) with CUDA events
+    # per-kernel timing of the three stage kinds (the dominant kernel) with CUDA events, the
+    # same kernel instantiations as the loop's (FP32: with the background-split tables)
     ctx = run.ctx
     dt_t = torch.tensor([float(stt.dt)], dtype=torch.float64, device=run.f.device)
     stage_ms = []
-    for stage, inp, fn, out in ((0, run.f, None, run.sa), (1, run.sa, run.f, run.sb),
-                                (2, run.sb, run.f, run.sa)):
-        for _ in range(2):
-            ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        for _ in range(reps):
-            ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
-        b.record()
-        torch.cuda.synchronize()
-        stage_ms.append(a.elapsed_time(b) / reps)
-    # field kernel (single CTA Poisson solve from a density)
+    ctx.set_background(run.background)
+    try:
+        for stage, inp, fn, out in ((0, run.f, None, run.sa), (1, run.sa, run.f, run.sb),
+                                    (2, run.sb, run.f, run.sa)):
+            for _ in range(2):
+                ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            for _ in range(reps):
+                ctx.rk_stage(stage, inp, fn, out, run.E, dt_t, partials=ctx.workspace)
+            b.record()
+            torch.cuda.synchronize()
+            stage_ms.append(a.elapsed_time(b) / reps)
+    finally:
+        ctx.set_background(None)
+    # field solve (one 8-CTA cluster: Poisson solve from a density)
     rho = torch.zeros((res[0], order), dtype=torch.float64, device=run.f.device)
     ctx.moment(run.f, rho)
     chg = (rho.mean() - rho).contiguous()
@@ -562,7 +567,7 @@ def main():
                    "buffers, 3 buffers)", "parallelism": f"replicas x{world}"},
         "roofline": head["roofline"],
         "e2e": head["e2e"],
-        # per step: 3 fused stage kernels + 3 single-CTA field solves; one moment per call
+        # per step: 3 fused stage kernels + 3 cluster field solves; one moment per call
         "gpu_launches": 6 * args.steps + 1,
         "clocks": ck,
         "variants": {"fp32_mixed": {"value": out["fp32"]["value"], "dtype": "f32",

@@ -233,7 +233,7 @@ struct FieldArgs {
     double kappa, dx, length, accel, bfield, umax, vmax, du, dv, courant;
 };
 
-constexpr int FIELD_THREADS = 1024;            // threads of the single-CTA field and scalar kernels
+constexpr int FIELD_THREADS = 1024;            // threads of the single-CTA scalar kernel
 constexpr int FIELD_MAX_NODES = 64 * NMAX;    // nx * n capacity of the shared buffers
 constexpr int FIELD_MAX_MODES = 2 * 160 + 1;  // M capacity
 

@@ -4,8 +4,8 @@ Mirrors ``Stepper`` and ``get_max_speeds`` of crewsdw/Vlasov1D2V (``main/timeste
 
 ``main_loop`` runs the nonlinear SSP-RK3 loop (``main/timestep.py:81-187``) on the device: per
 step three fused stage kernels (RHS + RK combination + moment partials of the result) and
-three single-CTA field kernels (density -> Poisson -> E, plus energy, dt and the loop
-bookkeeping after stage 2).  The loop state (dt, time, step count, "keep going" flag, energy
+three field solves, each one 8-CTA thread-block cluster (density -> Poisson -> E, plus energy,
+dt and the loop bookkeeping after stage 2).  The loop state (dt, time, step count, "keep going" flag, energy
 and time histories) lives in device memory, so batches of steps run without host syncs and,
 after the first batch, as a replayed CUDA graph.  The host reads the histories back once per
 batch and fills ``time_array`` / ``field_energy`` exactly as the reference's loop does,
