@@ -24,6 +24,7 @@
 #include "vlasov_stage_f32.cuh"
 #include "vlasov_field.cuh"
 #include "vlasov_stage_gen.cuh"
+#include "vlasov_gen_kinds.h"
 
 #include "vlasov_ctx.cuh"
 
@@ -429,8 +430,8 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                 if ((rc = gen_pair_bg_map<N, T>(c, a.bg_eu, &maps.bg_eu))) return rc;
                 if ((rc = gen_pair_bg_map<N, T>(c, a.bg_rb, &maps.bg_rb))) return rc;
             }
-            return check_launch(launch(c, vl::stage_gen_pair_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(),
-                                       s, a, tb, maps),
+            return check_launch(vl::gen_kinds_launch<T>(N, true, a.kind, a.bg_rb != nullptr, grid, G::smem_bytes(), s,
+                                                        a, tb, maps),
                                 "stage_gen_pair_kernel");
         }
     }
@@ -451,8 +452,8 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             if ((rc = gen_bg_map<N, T>(c, a.bg_eu, &maps.bg_eu))) return rc;
             if ((rc = gen_bg_map<N, T>(c, a.bg_rb, &maps.bg_rb))) return rc;
         }
-        return check_launch(launch(c, vl::stage_gen_tma_kernel<N, T>, grid, dim3(G::THREADS), G::smem_bytes(), s, a,
-                                   tb, maps),
+        return check_launch(vl::gen_kinds_launch<T>(N, false, a.kind, sizeof(T) == 4 && a.bg_rb != nullptr, grid,
+                                                    G::smem_bytes(), s, a, tb, maps),
                             "stage_gen_tma_kernel");
     }
     if (c->stage_kernel == VL_STAGE_GEN) {
@@ -515,6 +516,7 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool gpair) {
             const size_t smem = G::smem_bytes();
             cudaFuncSetAttribute(vl::stage_gen_pair_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
+            vl::gen_kinds_prepare<T>(N, true, smem);
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_pair_kernel<N, T>, G::THREADS,
                                                               smem) != cudaSuccess)
                 return 1;
@@ -525,6 +527,7 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool gpair) {
         using G = vl::GenTmaGeom<N, T>;
         const size_t smem = G::smem_bytes();
         cudaFuncSetAttribute(vl::stage_gen_tma_kernel<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        vl::gen_kinds_prepare<T>(N, false, smem);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_gen_tma_kernel<N, T>, G::THREADS,
                                                           smem) != cudaSuccess)
             return 1;

@@ -307,7 +307,7 @@ struct GenPair<float> {
 // partial [e][g][i] (of G per x element).  tb supplies up / xi / wu (compile-time j indices);
 // wfin[k] is the per-column factor of the moment partial (w_k / J_v for the single-problem
 // tables).  smem: GenGeom::smem_bytes() of dynamic shared memory, 128-byte aligned.
-template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PAIR = false>
+template <int N, typename T, int EPT, typename TB, bool TMA = false, bool PAIR = false, int KT = -1, int BT = -1>
 __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb, const double *wfin, int e,
                                                int g, int G, unsigned char *smem,
                                                const GenMaps *maps = nullptr) {
@@ -361,9 +361,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         El = e;
         Er = e + 2;
     }
-    const int kind = a.kind;
+    const int kind = KT >= 0 ? KT : a.kind;
     const bool with_fn = (kind == KIND_COMBINE);
-    const bool with_bg = GG::BG && a.bg_rb != nullptr;
+    const bool with_bg = GG::BG && (BT >= 0 ? BT == 1 : a.bg_rb != nullptr);
     const int nbt = (nv + EPT - 1) / EPT;
     const int tiles = nu * nbt;
     const int ntile = (g < tiles) ? (tiles - 1 - g) / G + 1 : 0;
@@ -520,6 +520,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     };
 
     const double accel = a.accel, bfield = a.bfield, nbfield = -a.bfield;
+    const float kvf = (float)(accel * nbfield);   // FP32 v speed per unit u
     const double dtd = (kind == KIND_RHS) ? 0.0 : *a.dt;
     const T dtT = (T)dtd, c0 = (T)a.c0, c1 = (T)a.c1, c2dt = (T)(a.c2 * dtd);
     const T jx = (T)a.jx, ju = (T)a.ju, jv = (T)a.jv;
@@ -644,12 +645,23 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
             const T uL0 = (sd0 >= 0.0) ? ufl.x : fu[0].x, uR0 = (sd0 >= 0.0) ? fu[N - 1].x : ufr.x;
             const T uL1 = (sd1 >= 0.0) ? ufl.y : fu[0].y, uR1 = (sd1 >= 0.0) ? fu[N - 1].y : ufr.y;
             T *pout = out + (size_t)Eg * sE_ + (size_t)i * sI + (size_t)Ag * sA + col;
+            float mf0 = 0.0f, mf1 = 0.0f;   // FP32: the tile's moment sums, added in FP64 after it
+            (void)mf0;
+            (void)mf1;
 #pragma unroll
             for (int j = 0; j < N; ++j) {
-                const double uxd = sUX[j];
-                const double svd = accel * (nbfield * uxd);
-                const bool xpos = uxd >= 0.0;
-                const bool vpos = svd >= 0.0;
+                // x and v speeds of row j (FP32: one conversion, the v speed formed in FP32)
+                T uxT, svT;
+                if constexpr (sizeof(T) == 4) {
+                    uxT = (float)sUX[j];
+                    svT = kvf * uxT;
+                } else {
+                    const double uxd = sUX[j];
+                    uxT = uxd;
+                    svT = accel * (nbfield * uxd);
+                }
+                const bool xpos = uxT >= (T)0;
+                const bool vpos = svT >= (T)0;
                 // x: sum_m up[i][m] F[m][j][k] + lifts
                 const T *pc = rowp(sIn, 0, j) + 2 * p;
                 T dx0 = (T)0, dx1 = (T)0;
@@ -702,7 +714,6 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 du0 = fma(-tb.xi[2 * j + 1], uR0, du0);
                 du1 = fma(tb.xi[2 * j], uL1, du1);
                 du1 = fma(-tb.xi[2 * j + 1], uR1, du1);
-                const T uxT = (T)uxd, svT = (T)svd;
                 T r0 = fma(uxT * dx0, jx, fma(sp0 * du0, ju, (svT * dv0) * jv));
                 T r1 = fma(uxT * dx1, jx, fma(sp1 * du1, ju, (svT * dv1) * jv));
                 if (with_bg) {   // RHS of the x-independent background
@@ -756,8 +767,17 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                         if (!pad1) gout[(size_t)(nx + 1) * sE_ + gb + 1] = fij.y;
                     }
                 }
-                mk0 = fma(tb.wu[j], (double)o.x, mk0);
-                mk1 = fma(tb.wu[j], (double)o.y, mk1);
+                if constexpr (sizeof(T) == 4) {
+                    mf0 = fmaf((float)tb.wu[j], o.x, mf0);
+                    mf1 = fmaf((float)tb.wu[j], o.y, mf1);
+                } else {
+                    mk0 = fma(tb.wu[j], (double)o.x, mk0);
+                    mk1 = fma(tb.wu[j], (double)o.y, mk1);
+                }
+            }
+            if constexpr (sizeof(T) == 4) {
+                mk0 += (double)mf0;
+                mk1 += (double)mf1;
             }
         };
         if (act) {
@@ -802,8 +822,10 @@ stage_gen_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb) {
     gen_stage_body<N, T, GenGeom<N, T>::EPT>(a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base);
 }
 
-// TMA form (16-byte-aligned state rows)
-template <int N, typename T>
+// TMA form (16-byte-aligned state rows).  KT / BT >= 0 fix the stage kind and the background
+// split at compile time (the instantiations launched by the loop: no per-row branches on them);
+// -1 reads them from the arguments.
+template <int N, typename T, int KT = -1, int BT = -1>
 __global__ void __launch_bounds__(GenTmaGeom<N, T>::THREADS, GenTmaGeom<N, T>::MINB)
 stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                      const __grid_constant__ GenMaps maps) {
@@ -811,12 +833,12 @@ stage_gen_tma_kernel(const StageArgs a, const __grid_constant__ StageTables<T> t
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
-    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true>(
+    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true, false, KT, BT>(
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
 }
 
-// paired-row TMA form (FP32 rows of R = 2 mod 4 floats)
-template <int N, typename T>
+// paired-row TMA form (FP32 rows of R = 2 mod 4 floats); KT / BT as for the TMA form
+template <int N, typename T, int KT = -1, int BT = -1>
 __global__ void __launch_bounds__(GenPairGeom<N, T>::THREADS, GenPairGeom<N, T>::MINB)
 stage_gen_pair_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                       const __grid_constant__ GenMaps maps) {
@@ -824,7 +846,7 @@ stage_gen_pair_kernel(const StageArgs a, const __grid_constant__ StageTables<T> 
     extern __shared__ __align__(16) unsigned char gen_smem_raw[];
     unsigned char *base = reinterpret_cast<unsigned char *>(
         (reinterpret_cast<uintptr_t>(gen_smem_raw) + 127) & ~(uintptr_t)127);
-    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true, true>(
+    gen_stage_body<N, T, GenGeom<N, T>::EPT, StageTables<T>, true, true, KT, BT>(
         a, tb, tb.wv, blockIdx.y, blockIdx.x, gridDim.x, base, &maps);
 }
 
