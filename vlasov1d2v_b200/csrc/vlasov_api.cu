@@ -401,12 +401,17 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             } else {
                 // FP64: combination stages stage an f^n tile; Euler / RHS stages take the form
                 // without it (3 CTAs per SM)
+                // (one instantiation per stage kind: no per-row branches on it)
                 if (a.kind == vl::KIND_COMBINE)
-                    return check_launch(launch(c, vl::stage_frag_kernel<T, true>, grid, dim3(G::THREADS),
-                                               G::smem_bytes(), s, a, tb, maps),
+                    return check_launch(launch(c, vl::stage_frag_kernel<T, true, vl::KIND_COMBINE>, grid,
+                                               dim3(G::THREADS), G::smem_bytes(), s, a, tb, maps),
                                         "stage_frag_kernel");
                 using G1 = vl::FragGeom<T, false>;
-                return check_launch(launch(c, vl::stage_frag_kernel<T, false>, grid, dim3(G1::THREADS),
+                if (a.kind == vl::KIND_EULER)
+                    return check_launch(launch(c, vl::stage_frag_kernel<T, false, vl::KIND_EULER>, grid,
+                                               dim3(G1::THREADS), G1::smem_bytes(), s, a, tb, maps),
+                                        "stage_frag_kernel");
+                return check_launch(launch(c, vl::stage_frag_kernel<T, false, vl::KIND_RHS>, grid, dim3(G1::THREADS),
                                            G1::smem_bytes(), s, a, tb, maps),
                                     "stage_frag_kernel");
             }
@@ -566,6 +571,8 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool gpair) {
             } else {
                 cudaFuncSetAttribute(vl::stage_frag_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem);
+                cudaFuncSetAttribute(vl::stage_frag_kernel<T, true, vl::KIND_COMBINE>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<T, true>,
                                                                   G::THREADS, smem) != cudaSuccess)
                     return 1;
@@ -601,6 +608,10 @@ int frag_nofn_occupancy() {
     const size_t smem = G::smem_bytes();
     cudaFuncSetAttribute(vl::stage_frag_kernel<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
+    cudaFuncSetAttribute(vl::stage_frag_kernel<double, false, vl::KIND_EULER>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(vl::stage_frag_kernel<double, false, vl::KIND_RHS>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_frag_kernel<double, false>, G::THREADS,
                                                       smem) != cudaSuccess)

@@ -115,7 +115,9 @@ struct Pair<float> {
     using V = float2;
 };
 
-template <typename T, bool WFN>
+// KT >= 0 fixes the stage kind at compile time (the instantiations the loop launches: no per-row
+// branches on it); -1 reads it from the arguments
+template <typename T, bool WFN, int KT = -1>
 __global__ void __launch_bounds__(FragGeom<T, WFN>::THREADS, FragGeom<T, WFN>::MINB)
 stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                   const __grid_constant__ FragMaps maps) {
@@ -154,7 +156,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
         El = e;
         Er = e + 2;
     }
-    const int kind = a.kind;
+    const int kind = KT >= 0 ? KT : a.kind;   // compile-time in the loop's instantiations
     const bool with_fn = WFN && (kind == KIND_COMBINE);   // combination stages launch the WFN form
     const bool with_bg = G::BG && a.bg_rb != nullptr;
     const uint32_t tx_bytes = G::TX_IN + 4 * G::TX_FACE + (with_fn ? G::TX_FN : 0) + (with_bg ? 2 * G::TX_BG : 0) +
@@ -242,6 +244,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
     }
     T *out = static_cast<T *>(a.out);
     T *gout = static_cast<T *>(a.ghost_out);
+    const bool ghost = gout != nullptr && (e == 0 || e == nx - 1);   // CTA-uniform
     double mk0 = 0.0, mk1 = 0.0;   // sum_j (w_j / J_u) out[.., j, k] for the two columns
 
     for (int q = 0; q < ntile_cta; ++q) {
@@ -394,7 +397,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                         o = fij;   // not reached: combination stages launch the WFN form
                     }
                     *reinterpret_cast<V2 *>(pout + j * sJ) = o;
-                    if (gout != nullptr) {
+                    if (ghost) {
                         // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
                         const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
                         if (e == nx - 1) *reinterpret_cast<V2 *>(gout + gb) = fij;

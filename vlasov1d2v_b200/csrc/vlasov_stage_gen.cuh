@@ -349,6 +349,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
     T *out = static_cast<T *>(a.out);
     T *gout = static_cast<T *>(a.ghost_out);
     const int nx = a.nx, nu = a.nu, nv = a.nv;
+    const bool ghost = gout != nullptr && (e == 0 || e == nx - 1);   // CTA-uniform
     const int U = nu + 2, V = nv + 2;
     const int sJ = V * N, sA = sJ * N, sI = sA * U;
     const size_t sE_ = (size_t)sI * N;
@@ -755,7 +756,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     po[0] = o.x;
                     if (!pad1) po[1] = o.y;
                 }
-                if (gout != nullptr) {
+                if (ghost) {
                     // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
                     const size_t gb = (size_t)i * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
                     if (e == nx - 1) {
