@@ -288,16 +288,23 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
             T *pout = out + obase;
             const T *prow = sIn + g * PS + P + wc;   // row slice F[g][j][element] at j = 0
             // the warp's j rows (compile-time j: table constants)
-            auto rows = [&](auto j0c) {
+            // upwind directions of x (sign of u J_x) and v (sign of a (-B u) J_v) at the element's end
+            // rows: the same for every j of a u element that does not straddle u = 0, and then the
+            // direction-dependent fragments and coefficients are chosen once per tile
+            const V2 usF = sUS[0], usL = sUS[N - 1];
+            const bool xpos0 = usF.x >= (T)0, vpos0 = usF.y >= (T)0;
+            const bool uni = (xpos0 == (usL.x >= (T)0)) && (vpos0 == (usL.y >= (T)0));
+            auto rows = [&](auto j0c, auto uni_c) {
                 constexpr int J0 = decltype(j0c)::value;
+                constexpr bool UNI = decltype(uni_c)::value;
 #pragma unroll
                 for (int jj = 0; jj < G::NJ; ++jj) {
                     const int j = J0 + jj;
                     // x and v flux speeds (their signs are the upwind directions) times the
                     // direction weights
                     const V2 us = sUS[j];
-                    const bool xpos = us.x >= (T)0;
-                    const bool vpos = us.y >= (T)0;
+                    const bool xpos = UNI ? xpos0 : us.x >= (T)0;
+                    const bool vpos = UNI ? vpos0 : us.y >= (T)0;
                     const T uxj = us.x * jx, svj = us.y * jv;
                     T dx0, dx1, dv0, dv1;
                     if constexpr (G::MMA) {
@@ -407,14 +414,20 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                     mk1 = fma(tb.wu[j], (double)o.y, mk1);
                 }
             };
+            auto rows_j = [&](auto j0c) {
+                if (uni)
+                    rows(j0c, std::true_type{});
+                else
+                    rows(j0c, std::false_type{});
+            };
             if constexpr (G::JS == 1) {
-                rows(std::integral_constant<int, 0>{});
+                rows_j(std::integral_constant<int, 0>{});
             } else {
                 static_assert(G::JS == 2, "one or two warps per v element");
                 if (h == 0)
-                    rows(std::integral_constant<int, 0>{});
+                    rows_j(std::integral_constant<int, 0>{});
                 else
-                    rows(std::integral_constant<int, G::NJ>{});
+                    rows_j(std::integral_constant<int, G::NJ>{});
             }
         }
         __syncthreads();   // stage s fully consumed
