@@ -284,6 +284,27 @@ def measured_peak_hbm():
         return 6650.0, "fallback 6.65 TB/s (of fallback)"
 
 
+def capture_steps(run, steps):
+    """CUDA graph of `steps` SSP-RK3 steps of a Stepper run.  The FP32 mixed form's
+    background-split tables are installed on the context while the graph is captured, so the
+    captured stage kernels carry them, as in Stepper launches."""
+    import torch
+
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    run.ctx.set_background(run.background)
+    try:
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                run.ctx.ssp_rk3_steps(run.f, run.sa, run.sb, run.E, run.phi, run.state, steps)
+    finally:
+        run.ctx.set_background(None)
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    return g
+
+
 def measure_precision(precision, steps, warmup, reps, dist, res=None, order=None, e2e=True):
     import torch
 
@@ -306,14 +327,7 @@ def measure_precision(precision, steps, warmup, reps, dist, res=None, order=None
     if warmup:
         run.launch(warmup, use_graph=False)
     torch.cuda.synchronize()
-    g = torch.cuda.CUDAGraph()
-    s = torch.cuda.Stream()
-    s.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(s):
-        with torch.cuda.graph(g, stream=s):
-            run.ctx.ssp_rk3_steps(run.f, run.sa, run.sb, run.E, run.phi, run.state, steps)
-    torch.cuda.current_stream().wait_stream(s)
-    torch.cuda.synchronize()
+    g = capture_steps(run, steps)
 
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     dist.barrier()
