@@ -196,6 +196,14 @@ VL_API int vl_ssp_rk3_steps(vl_ctx *ctx, void *f, void *stage_a, void *stage_b, 
  * the split off.  FP32 contexts only.                                                         */
 VL_API int vl_set_background(vl_ctx *ctx, const float *rb, const float *eu);
 
+/* Optional, with vl_set_background: the same two tables interleaved per column pair,
+ *   pairs[r][p] = {eu[r][2p], eu[r][2p+1], rb[r][2p], rb[r][2p+1]},  r over the (nu+2) n rows,
+ * p over the (nv+2) n / 2 column pairs (16-byte aligned, caller-owned, kept until the next call).
+ * The order-8 FP32 stage kernel then stages both tables with one tensor copy and reads them with
+ * one 128-bit load per row.  NULL clears it; vl_set_background(ctx, NULL, NULL) clears it too.
+ * FP32 contexts with an even (nv+2) n only.                                                     */
+VL_API int vl_set_background_pairs(vl_ctx *ctx, const float *pairs);
+
 /* Copy f's ghost elements (all six ghost slabs) into a stage buffer and perform the
  * reference's periodic x-ghost swap on f (Distribution.swap_ghost_cells_of_array,
  * main/grid.py:187-189).  Call once before a run and after f is replaced.                  */

@@ -25,7 +25,7 @@ EXPORTED = (
     "vl_workspace_bytes", "vl_rhs", "vl_rhs_weighted", "vl_moment", "vl_poisson", "vl_field_energy", "vl_adapt_dt",
     "vl_rk_stage", "vl_run_state_init", "vl_ssp_rk3_steps", "vl_sync_ghosts",
     "vl_ssp_rk3_steps_noalloc", "vl_initial_state", "vl_smooth_edges", "vl_interpolate",
-    "vl_set_background", "vl_ens_create", "vl_ens_destroy", "vl_ens_workspace_bytes", "vl_ens_bind",
+    "vl_set_background", "vl_set_background_pairs", "vl_ens_create", "vl_ens_destroy", "vl_ens_workspace_bytes", "vl_ens_bind",
     "vl_ens_schedule", "vl_ens_schedule_by_order", "vl_ens_commit", "vl_ens_steps", "vl_mlp_dims", "vl_mlp_forward",
     "vl_mlp_partial_floats", "vl_mlp_backward", "vl_mlp_adam", "vl_closure_features", "vl_closure_apply",
     "vl_poisson_dg", "vl_axpby_interior",
@@ -105,6 +105,7 @@ def _declare(lib):
     lib.vl_ssp_rk3_steps_noalloc.argtypes = [vp, vp, vp, vp, vp, vp, vp, i, vp]
     i32 = ctypes.c_int32
     lib.vl_set_background.argtypes = [vp, vp, vp]
+    lib.vl_set_background_pairs.argtypes = [vp, vp]
     lib.vl_poisson_dg.argtypes = [vp, vp, vp, vp, vp, i32, vp, vp, vp]
     lib.vl_axpby_interior.argtypes = [vp, vp, vp, ctypes.c_double, ctypes.c_double, vp]
     lib.vl_ens_create.argtypes = [ctypes.POINTER(vp), i32, ctypes.POINTER(vp)]

@@ -177,6 +177,8 @@ class NativeContext:
             _lib.call("vl_set_background", self.handle, None, None)
         else:
             _lib.call("vl_set_background", self.handle, _ptr(tables["rb"]), _ptr(tables["eu"]))
+            pairs = tables.get("pairs")
+            _lib.call("vl_set_background_pairs", self.handle, None if pairs is None else _ptr(pairs))
 
     def sync_ghosts(self, f, stage):
         self._check_state(f, "f")

@@ -170,6 +170,33 @@ int bg_map(vl_ctx *c, const float *ptr, int n, CUtensorMap *out) {
     return VL_OK;
 }
 
+// 2-D view [U n][V n / 2 pairs x 4] of the background tables interleaved per column pair (FP32,
+// n = 8 kernel), box (2 COLS, n): one tile's rows of both tables
+int bg_pair_map(vl_ctx *c, const float *ptr, int n, CUtensorMap *out) {
+    auto key = std::make_pair(static_cast<const void *>(ptr), 9);
+    auto it = c->maps.find(key);
+    if (it != c->maps.end()) {
+        *out = it->second;
+        return VL_OK;
+    }
+    auto enc = encode_fn();
+    if (!enc) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t U = c->cfg.nu + 2, V = c->cfg.nv + 2;
+    cuuint64_t dims[2] = {2 * V * n, U * n};
+    cuuint64_t strides[1] = {2 * V * n * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)(2 * vl::FragGeom<float>::COLS), (cuuint32_t)n};
+    cuuint32_t estr[2] = {1, 1};
+    CUtensorMap m;
+    CUresult r = enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(VL_ERR_CUDA, "cuTensorMapEncodeTiled (background pair table) failed");
+    if (c->maps.size() > 64) c->maps.clear();
+    c->maps[key] = m;
+    *out = m;
+    return VL_OK;
+}
+
 // 5-D view of a state for the generic kernel's TMA form: which 0 = tile (WB, RJ, 1, n, 1),
 // 1 = x-node plane (WB, n, 1, 1, 1), 2 = j row of every x node (WB, 1, 1, n, 1)
 template <int N, typename T>
@@ -365,7 +392,11 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
             if ((rc = state_map<N, T>(c, a.in, 1, &maps.in_xface))) return rc;
             if ((rc = state_map<N, T>(c, a.in, 2, &maps.in_uface))) return rc;
             if ((rc = state_map<N, T>(c, a.fn ? a.fn : a.in, 7, &maps.fn_tile))) return rc;
-            if (G::BG && a.bg_rb != nullptr) {
+            if (G::BG && a.bg_rb != nullptr && c->bg_pair != nullptr) {
+                // the two tables interleaved per column pair: one (2 COLS, n) box per tile
+                if ((rc = bg_pair_map(c, c->bg_pair, N, &maps.bg_eu))) return rc;
+                std::memset(&maps.bg_rb, 0, sizeof(maps.bg_rb));
+            } else if (G::BG && a.bg_rb != nullptr) {
                 if ((rc = bg_map(c, a.bg_eu, N, &maps.bg_eu))) return rc;
                 if ((rc = bg_map(c, a.bg_rb, N, &maps.bg_rb))) return rc;
             } else {
@@ -378,23 +409,26 @@ int launch_stage_t(vl_ctx *c, const vl::StageArgs &a0, cudaStream_t s) {
                 a.sx = a.jx / c->cfg.jx;
                 a.sv = a.jv / c->cfg.jv;
                 const vl::F32Tables &ft = f32_tables(c);
-                const bool bg = a.bg_rb != nullptr;
+                // background split: 0 none, 1 two tables, 2 the interleaved pair table
+                const int bg = a.bg_rb == nullptr ? 0 : (c->bg_pair != nullptr ? 2 : 1);
                 const dim3 blk(G::THREADS);
                 const size_t sm = G::smem_bytes();
+                auto go = [&](auto kc) {
+                    constexpr int K = decltype(kc)::value;
+                    if (bg == 2) return launch(c, vl::stage_f32_kernel<K, 2>, grid, blk, sm, s, a, ft, maps);
+                    if (bg == 1) return launch(c, vl::stage_f32_kernel<K, 1>, grid, blk, sm, s, a, ft, maps);
+                    return launch(c, vl::stage_f32_kernel<K, 0>, grid, blk, sm, s, a, ft, maps);
+                };
                 cudaError_t le;
                 switch (a.kind) {
                     case vl::KIND_EULER:
-                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_EULER, true>, grid, blk, sm, s, a, ft, maps)
-                                : launch(c, vl::stage_f32_kernel<vl::KIND_EULER, false>, grid, blk, sm, s, a, ft, maps);
+                        le = go(std::integral_constant<int, vl::KIND_EULER>{});
                         break;
                     case vl::KIND_COMBINE:
-                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_COMBINE, true>, grid, blk, sm, s, a, ft, maps)
-                                : launch(c, vl::stage_f32_kernel<vl::KIND_COMBINE, false>, grid, blk, sm, s, a, ft,
-                                         maps);
+                        le = go(std::integral_constant<int, vl::KIND_COMBINE>{});
                         break;
                     default:
-                        le = bg ? launch(c, vl::stage_f32_kernel<vl::KIND_RHS, true>, grid, blk, sm, s, a, ft, maps)
-                                : launch(c, vl::stage_f32_kernel<vl::KIND_RHS, false>, grid, blk, sm, s, a, ft, maps);
+                        le = go(std::integral_constant<int, vl::KIND_RHS>{});
                         break;
                 }
                 return check_launch(le, "stage_f32_kernel");
@@ -553,19 +587,19 @@ int stage_occupancy_t(bool tma, bool frag, bool gen, bool gtma, bool gpair) {
             const size_t smem = G::smem_bytes();
             if constexpr (sizeof(T) == 4) {
                 // every instantiation of the FP32 kernel takes the same dynamic shared memory
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_EULER, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_EULER, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_COMBINE, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_COMBINE, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_RHS, true>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                cudaFuncSetAttribute(vl::stage_f32_kernel<vl::KIND_RHS, false>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_f32_kernel<vl::KIND_COMBINE, true>,
+                auto attr = [&](auto kc) {
+                    constexpr int K = decltype(kc)::value;
+                    cudaFuncSetAttribute(vl::stage_f32_kernel<K, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+                    cudaFuncSetAttribute(vl::stage_f32_kernel<K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+                    cudaFuncSetAttribute(vl::stage_f32_kernel<K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+                };
+                attr(std::integral_constant<int, vl::KIND_EULER>{});
+                attr(std::integral_constant<int, vl::KIND_COMBINE>{});
+                attr(std::integral_constant<int, vl::KIND_RHS>{});
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, vl::stage_f32_kernel<vl::KIND_COMBINE, 1>,
                                                                   G::THREADS, smem) != cudaSuccess)
                     return 1;
             } else {
@@ -1160,6 +1194,17 @@ int vl_run_state_init(vl_ctx *c, vl_run_state *state, const double *E0, double f
     return check_launch("scalars_kernel(init)");
 }
 
+int vl_set_background_pairs(vl_ctx *c, const float *pairs) {
+    if (!c) return fail(VL_ERR_INVALID, "null context");
+    if (pairs && c->cfg.precision != VL_FP32)
+        return fail(VL_ERR_UNSUPPORTED, "the background split is a form of the FP32 context");
+    if (pairs && (((c->cfg.nv + 2) * c->cfg.n) % 2 != 0))
+        return fail(VL_ERR_INVALID, "background pair table needs an even row length (nv+2) n");
+    if (reinterpret_cast<uintptr_t>(pairs) & 15) return fail(VL_ERR_INVALID, "background pair table must be 16-byte aligned");
+    c->bg_pair = pairs;
+    return VL_OK;
+}
+
 int vl_set_background(vl_ctx *c, const float *rb, const float *eu) {
     if (!c) return fail(VL_ERR_INVALID, "null context");
     if ((rb == nullptr) != (eu == nullptr)) return fail(VL_ERR_INVALID, "background tables: give both or none");
@@ -1169,6 +1214,7 @@ int vl_set_background(vl_ctx *c, const float *rb, const float *eu) {
         return fail(VL_ERR_INVALID, "background tables must be 16-byte aligned");
     c->bg_rb = rb;
     c->bg_eu = eu;
+    if (rb == nullptr) c->bg_pair = nullptr;   // the pair table belongs to the split
     return VL_OK;
 }
 

@@ -45,6 +45,7 @@ struct vl_ctx {
     bool gen_pair = false;        // generic stage kernel in its paired-row TMA form (FP32, R = 2 mod 4)
     const float *bg_rb = nullptr;   // background-split RHS tables (caller-owned)
     const float *bg_eu = nullptr;
+    const float *bg_pair = nullptr; // the same tables interleaved per column pair (caller-owned, optional)
     std::map<std::pair<const void *, int>, CUtensorMap> maps;   // tensor maps per buffer
     vl::F32Tables f32_tables;       // FP32 n = 8 kernel's coefficient pairs (built on first use)
     bool f32_tables_ready = false;

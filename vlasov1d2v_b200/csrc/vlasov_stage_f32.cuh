@@ -19,7 +19,9 @@
 // u element straddles zero take the same body with the selection made per j.  The u direction
 // (sign of a (E_i + B v_k)) is fixed per thread and tile.  The moment partial of the output is
 // accumulated per tile in FP32 pairs over the tile's eight j, then added in FP64.
-// Stage kinds and the background split are template parameters: no per-row branches.
+// Stage kinds and the background split are template parameters: no per-row branches.  BG 0: no
+// split; 1: the eu and rb RHS tables as two 2-D boxes; 2: the two tables interleaved per column
+// pair ({eu(k), eu(k+1), rb(k), rb(k+1)}), one box and one 128-bit load per row.
 #pragma once
 
 #include <cuda.h>
@@ -51,8 +53,10 @@ __device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(
 __device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 
-template <int KIND, bool BG>
+template <int KIND, int BG>
 __global__ void __launch_bounds__(FragGeom<float>::THREADS, FragGeom<float>::MINB)
 stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const __grid_constant__ FragMaps maps) {
     using G = FragGeom<float>;
@@ -94,7 +98,7 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
         Er = e + 2;
     }
     constexpr bool WITH_FN = (KIND == KIND_COMBINE);
-    constexpr uint32_t TX = G::TX_IN + 4 * G::TX_FACE + (WITH_FN ? G::TX_FN : 0) + (BG ? 2 * G::TX_BG : 0) +
+    constexpr uint32_t TX = G::TX_IN + 4 * G::TX_FACE + (WITH_FN ? G::TX_FN : 0) + (BG != 0 ? 2 * G::TX_BG : 0) +
                             (uint32_t)sizeof(float4) * N;
     static_assert(sizeof(float4) * N <= G::UX_B, "u-node speed slot");
     const int nbt = (nv + EPT - 1) / EPT;
@@ -127,10 +131,12 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
         if constexpr (WITH_FN) tma_load_5d(st + G::IN_B, &maps.fn_tile, &full[s], x0 - P, 0, Ag, 0, Eg);
         bulk_load(uf + G::UF_B + G::BG_B, static_cast<const float4 *>(a.usv) + Ag * N,
                   (uint32_t)sizeof(float4) * N, &full[s]);
-        if constexpr (BG) {
+        if constexpr (BG == 1) {
             unsigned char *bg = uf + G::UF_B;
             tma_load_2d(bg, &maps.bg_eu, &full[s], x0, Ag * N);
             tma_load_2d(bg + sizeof(float) * COLS * N, &maps.bg_rb, &full[s], x0, Ag * N);
+        } else if constexpr (BG == 2) {
+            tma_load_2d(uf + G::UF_B, &maps.bg_eu, &full[s], 2 * x0, Ag * N);   // (2 COLS, n) box
         }
     };
     if (tid == 0) {
@@ -284,10 +290,13 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
                     float2 r = fmul2(f2(us.z, us.w), dv);
                     r = ffma2(spu, du, r);
                     r = ffma2(f2(us.x, us.y), dx, r);
-                    if constexpr (BG) {
+                    if constexpr (BG == 1) {
                         const float2 eu = lds2(sBG + j * COLS + cl);
                         const float2 rb = lds2(sBG + N * COLS + j * COLS + cl);
                         r = fadd2(r, ffma2(Ei2, eu, rb));
+                    } else if constexpr (BG == 2) {
+                        const float4 er = lds4(sBG + j * 2 * COLS + 2 * cl);   // {eu, eu', rb, rb'}
+                        r = fadd2(r, ffma2(Ei2, lo2(er), hi2(er)));
                     }
                     const float2 fij = fu[j];
                     float2 o;

@@ -12,8 +12,10 @@
 // with the own-trace part of each upwind lift folded into the up fragments selected by the sign
 // of the speed (upP / upM) and the neighbour trace added by one FMA per output.  The u contraction
 // mixes the j of one thread's own outputs and runs on the FMA pipes from a per-thread copy of
-// F[i][0..7][k..k+1].  The FP32 form runs all three contractions on the FMA pipes in the
-// same layout.
+// F[i][0..7][k..k+1].  The row loop is instantiated per stage kind and for uniform upwind
+// directions over the tile (a u element that does not straddle u = 0: fragments and face planes
+// chosen once per tile) or per-row directions, so it branches on neither.  FP32 states at n = 8
+// run the packed-FP32 kernel (vlasov_stage_f32.cuh) on this file's FragGeom<float> stage layout.
 //
 // Shared-memory stage (one TMA box each, no multicast):
 //   IN [i][9][36 | 40]   stage input incl. pad columns (v traces) and one zero-filled row:

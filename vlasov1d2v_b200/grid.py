@@ -263,6 +263,11 @@ class Distribution:
         dev = _device.device()
         out = {k: torch.as_tensor(np.ascontiguousarray(v), dtype=torch.float32, device=dev)
                for k, v in tabs.items()}
+        rows, cols = f0.shape[0] * f0.shape[1], f0.shape[2] * f0.shape[3]
+        if cols % 2 == 0:   # both tables interleaved per column pair (vl_set_background_pairs)
+            eu2 = out["eu"].reshape(rows, cols // 2, 2)
+            rb2 = out["rb"].reshape(rows, cols // 2, 2)
+            out["pairs"] = torch.cat([eu2, rb2], dim=2).contiguous()
         self._bg_cache[key] = out
         return out
 
