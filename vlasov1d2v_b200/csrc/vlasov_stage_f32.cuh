@@ -231,8 +231,9 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
             const float4 us0 = sUS[0], us7 = sUS[N - 1];
             const bool uni = ((us0.x >= 0.0f) == (us7.x >= 0.0f)) && ((us0.z >= 0.0f) == (us7.z >= 0.0f));
             float2 mk = f2s(0.0f);
-            auto rows = [&](auto uni_c) {
+            auto rows = [&](auto uni_c, auto ghost_c) {
                 constexpr bool UNI = decltype(uni_c)::value;
+                constexpr bool GHOST = decltype(ghost_c)::value;   // x-ghost refresh rows
                 // folded coefficients for the tile (uniform directions)
                 float2 cxn = f2s(0.0f);
                 const float *sXn = sXF;
@@ -310,7 +311,7 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
                         o = ffma2(c2dt2, r, ffma2(c12, ffma2(mone, fnv, fij), fnv));
                     }
                     *reinterpret_cast<float2 *>(pout + (size_t)j * sJ) = o;
-                    if (ghost) {
+                    if constexpr (GHOST) {
                         // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
                         const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
                         if (e == nx - 1) *reinterpret_cast<float2 *>(gout + gb) = fij;
@@ -319,10 +320,19 @@ stage_f32_kernel(const StageArgs a, const __grid_constant__ F32Tables tb, const 
                     mk = ffma2(tb.wu2[j], o, mk);
                 }
             };
-            if (uni)
-                rows(std::true_type{});
-            else
-                rows(std::false_type{});
+            // (the edge x elements of stage 1 refresh f's ghost slabs: their own instantiation, so
+            // the other CTAs' row loop has no branch on it)
+            if (ghost) {
+                if (uni)
+                    rows(std::true_type{}, std::true_type{});
+                else
+                    rows(std::false_type{}, std::true_type{});
+            } else {
+                if (uni)
+                    rows(std::true_type{}, std::false_type{});
+                else
+                    rows(std::false_type{}, std::false_type{});
+            }
             mk0 += (double)mk.x;
             mk1 += (double)mk.y;
         }

@@ -296,7 +296,8 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
             const V2 usF = sUS[0], usL = sUS[N - 1];
             const bool xpos0 = usF.x >= (T)0, vpos0 = usF.y >= (T)0;
             const bool uni = (xpos0 == (usL.x >= (T)0)) && (vpos0 == (usL.y >= (T)0));
-            auto rows = [&](auto j0c, auto uni_c) {
+            auto rows = [&](auto j0c, auto uni_c, auto ghost_c) {
+                constexpr bool GHOST = decltype(ghost_c)::value;   // x-ghost refresh rows
                 constexpr int J0 = decltype(j0c)::value;
                 constexpr bool UNI = decltype(uni_c)::value;
 #pragma unroll
@@ -406,7 +407,7 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                         o = fij;   // not reached: combination stages launch the WFN form
                     }
                     *reinterpret_cast<V2 *>(pout + j * sJ) = o;
-                    if (ghost) {
+                    if constexpr (GHOST) {
                         // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
                         const size_t gb = (size_t)g * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
                         if (e == nx - 1) *reinterpret_cast<V2 *>(gout + gb) = fij;
@@ -417,10 +418,18 @@ stage_frag_kernel(const StageArgs a, const __grid_constant__ StageTables<T> tb,
                 }
             };
             auto rows_j = [&](auto j0c) {
-                if (uni)
-                    rows(j0c, std::true_type{});
-                else
-                    rows(j0c, std::false_type{});
+                // (the edge x elements of stage 1 refresh f's ghost slabs: their own instantiation)
+                if (ghost) {
+                    if (uni)
+                        rows(j0c, std::true_type{}, std::true_type{});
+                    else
+                        rows(j0c, std::false_type{}, std::true_type{});
+                } else {
+                    if (uni)
+                        rows(j0c, std::true_type{}, std::false_type{});
+                    else
+                        rows(j0c, std::false_type{}, std::false_type{});
+                }
             };
             if constexpr (G::JS == 1) {
                 rows_j(std::integral_constant<int, 0>{});
