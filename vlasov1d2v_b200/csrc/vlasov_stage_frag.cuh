@@ -14,7 +14,8 @@
 // mixes the j of one thread's own outputs and runs on the FMA pipes from a per-thread copy of
 // F[i][0..7][k..k+1].  The row loop is instantiated per stage kind and for uniform upwind
 // directions over the tile (a u element that does not straddle u = 0: fragments and face planes
-// chosen once per tile) or per-row directions, so it branches on neither.  FP32 states at n = 8
+// chosen once per tile) or per-row directions, and for the x-ghost-refresh rows of the edge x
+// elements of stage 1 apart from the others, so it branches on none of these.  FP32 states at n = 8
 // run the packed-FP32 kernel (vlasov_stage_f32.cuh) on this file's FragGeom<float> stage layout.
 //
 // Shared-memory stage (one TMA box each, no multicast):

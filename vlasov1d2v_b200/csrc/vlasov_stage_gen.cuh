@@ -607,8 +607,9 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
         };
         // the tile body, for the parity RP of the tile's first row among the U n rows (paired form;
         // 0 otherwise): row r of the tile is row (RP + r) / 2 of parity (RP + r) % 2
-        auto tile_rows = [&](auto rpc) {
+        auto tile_rows = [&](auto rpc, auto ghost_c) {
             constexpr int RP = decltype(rpc)::value;
+            constexpr bool GHOST = decltype(ghost_c)::value;   // x-ghost refresh rows
             (void)RP;
             // IN / FN layout: pointer to node 0 of element b in row r of plane pl
             auto rowp = [&](const T *arr, int pl, int r) -> const T * {
@@ -756,7 +757,7 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                     po[0] = o.x;
                     if (!pad1) po[1] = o.y;
                 }
-                if (ghost) {
+                if constexpr (GHOST) {
                     // periodic x-ghost refresh of f (Distribution.swap_ghost_cells_of_array)
                     const size_t gb = (size_t)i * sI + (size_t)Ag * sA + (size_t)j * sJ + col;
                     if (e == nx - 1) {
@@ -781,14 +782,22 @@ __device__ __forceinline__ void gen_stage_body(const StageArgs &a, const TB &tb,
                 mk1 += (double)mf1;
             }
         };
+        // (the edge x elements of stage 1 refresh f's ghost slabs: their own instantiation, so the
+        // other CTAs' row loop has no branch on it)
+        auto tile_ghost = [&](auto rpc) {
+            if (ghost)
+                tile_rows(rpc, std::true_type{});
+            else
+                tile_rows(rpc, std::false_type{});
+        };
         if (act) {
             if constexpr (PAIR) {
                 if ((Ag * N) & 1)
-                    tile_rows(std::integral_constant<int, 1>{});
+                    tile_ghost(std::integral_constant<int, 1>{});
                 else
-                    tile_rows(std::integral_constant<int, 0>{});
+                    tile_ghost(std::integral_constant<int, 0>{});
             } else {
-                tile_rows(std::integral_constant<int, 0>{});
+                tile_ghost(std::integral_constant<int, 0>{});
             }
         }
         __syncthreads();   // stage q % NST consumed before it is refilled
