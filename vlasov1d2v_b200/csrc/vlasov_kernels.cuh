@@ -154,7 +154,10 @@ struct MomentArgs {
 };
 
 constexpr int MOMENT_THREADS = 256;
-constexpr int MOMENT_CTAS_PER_SM = 4;
+// 2 resident CTAs per SM leave 128 registers per thread, room for most of a column's n x n loads
+// in flight at once (at 4 CTAs, 64 registers, the loads issued a few at a time and the kernel ran
+// at half the HBM rate, bound by load latency)
+constexpr int MOMENT_CTAS_PER_SM = 2;
 
 template <int N, typename T>
 __global__ void __launch_bounds__(MOMENT_THREADS, MOMENT_CTAS_PER_SM) moment_kernel(const MomentArgs a) {
