@@ -7,6 +7,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <map>
@@ -779,6 +780,7 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     a.du = c->cfg.du;
     a.dv = c->cfg.dv;
     a.courant = c->cfg.courant;
+    a.prefetch = vl::field_solve_smem(a.n, a.M) + vl::field_prefetch_bytes(a.nx, a.n, a.M) <= vl::FIELD_DYN_SMEM_MAX;
     return a;
 }
 
@@ -788,7 +790,8 @@ int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3(vl::FC);
     cfg.blockDim = dim3(vl::FS_THREADS);
-    cfg.dynamicSmemBytes = vl::field_solve_smem(c->cfg.n, c->cfg.n_modes);
+    cfg.dynamicSmemBytes = vl::field_solve_smem(c->cfg.n, c->cfg.n_modes) +
+                           (a.prefetch ? vl::field_prefetch_bytes(c->cfg.nx, c->cfg.n, c->cfg.n_modes) : 0);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -959,8 +962,9 @@ int vl_ctx_create(const vl_config *cfg, vl_ctx **out) {
         return cleanup(rc);
     if ((rc = upload(&c->d_qnode, cfg->dft_qnode, nm))) return cleanup(rc);
     {
-        const cudaError_t ee = cudaFuncSetAttribute(vl::field_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                    (int)vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES));
+        const cudaError_t ee = cudaFuncSetAttribute(
+            vl::field_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            (int)std::max(vl::field_solve_smem(vl::NMAX, vl::FIELD_MAX_MODES), vl::FIELD_DYN_SMEM_MAX));
         if (ee != cudaSuccess) return cleanup(cuda_fail(ee, "cudaFuncSetAttribute(field_solve_kernel)"));
     }
     {

@@ -37,6 +37,23 @@ constexpr int FS_THREADS = 256;     // threads per CTA
 // dynamic shared memory of one CTA: C_E and C_P, [n][M] complex each
 __host__ __device__ constexpr size_t field_solve_smem(int n, int M) { return sizeof(double2) * (size_t)2 * n * M; }
 
+// the phase-table entries one CTA reads in its loops: the columns of its modes for every element
+// (forward transform) and the rows of the elements that hold its nodes (inverse transform)
+__host__ __device__ constexpr int field_fwd_cols(int M) { return (M + FC - 1) / FC; }
+__host__ __device__ constexpr int field_inv_rows(int nx, int n) { return ((nx * n + FC - 1) / FC + n - 1) / n + 1; }
+__host__ __device__ constexpr size_t field_prefetch_bytes(int nx, int n, int M) {
+    return sizeof(double2) * ((size_t)nx * field_fwd_cols(M) + (size_t)field_inv_rows(nx, n) * M);
+}
+// dynamic shared memory the loop's field solves may take with the prefetch (the kernel's static
+// shared memory is about 20 KB)
+constexpr size_t FIELD_DYN_SMEM_MAX = 200 * 1024;
+
+__device__ __forceinline__ void field_cp16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+
 __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
@@ -59,6 +76,24 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     if (!go) return;   // the whole cluster returns: no barrier is left waiting
     double2 *sCE = fs_dyn;
     double2 *sCP = fs_dyn + (size_t)n * M;
+    const int Mc = field_fwd_cols(M);
+    const int m0 = rank * Mc;
+    const int Nc = (nn + FC - 1) / FC;
+    const int p0 = rank * Nc;
+    // elements holding this rank's nodes [p0, min(p0 + Nc, nn))
+    const int e_lo = p0 < nn ? p0 / n : 0;
+    const int e_hi = p0 < nn ? (min(p0 + Nc, nn) - 1) / n : -1;
+    double2 *sPF = sCP + (size_t)n * M;            // [nx][Mc]: phase[e][m0 + ml]
+    double2 *sPI = sPF + (size_t)nx * Mc;          // [e_hi - e_lo + 1][M]: phase rows of e_lo..e_hi
+    if (a.prefetch) {
+        for (int q = tid; q < nx * Mc; q += blockDim.x) {
+            const int e = q / Mc, ml = q - e * Mc;
+            if (m0 + ml < M) field_cp16(sPF + q, a.phase + (size_t)e * M + m0 + ml);
+        }
+        const int rows = e_hi - e_lo + 1;
+        for (int q = tid; q < rows * M; q += blockDim.x) field_cp16(sPI + q, a.phase + (size_t)e_lo * M + q);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    }
 
     // 1. charge (every CTA, identical)
     if (a.charge_in != nullptr) {
@@ -83,9 +118,11 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
         __syncthreads();
     }
 
+    if (a.prefetch) {   // the copies of every thread are in shared memory
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+    }
     // 2. forward over this rank's modes: thread (mode slot ml, element range part)
-    const int Mc = (M + FC - 1) / FC;
-    const int m0 = rank * Mc;
     const int parts = FS_THREADS / Mc > 0 ? FS_THREADS / Mc : 1;   // element ranges per mode
     {
         const int ml = tid % Mc, part = tid / Mc;
@@ -106,7 +143,7 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
                         si = fma(r, ell[j].y, si);
                     }
                 }
-                const double2 ph = a.phase[(size_t)e * M + m];
+                const double2 ph = a.prefetch ? sPF[e * Mc + ml] : a.phase[(size_t)e * M + m];
                 cr = fma(ph.x, sr, fma(-ph.y, si, cr));
                 ci = fma(ph.x, si, fma(ph.y, sr, ci));
             }
@@ -153,8 +190,6 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     __syncthreads();
 
     // 4. inverse over this rank's nodes: thread (node slot, mode range part)
-    const int Nc = (nn + FC - 1) / FC;
-    const int p0 = rank * Nc;
     const int iparts = FS_THREADS / Nc > 0 ? FS_THREADS / Nc : 1;
     const int slots = FS_THREADS / iparts;   // node slots per pass
     vl_run_state *st = a.state;
@@ -165,7 +200,7 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
         double er = 0.0, pr = 0.0;
         if (part < iparts && pl < Nc && p < nn) {
             const int e = p / n, j = p - e * n;
-            const double2 *ph = a.phase + (size_t)e * M;
+            const double2 *ph = a.prefetch ? sPI + (size_t)(e - e_lo) * M : a.phase + (size_t)e * M;
             const double2 *ce = sCE + (size_t)j * M;
             const double2 *cp = sCP + (size_t)j * M;
             const int mb = (part * M) / iparts, me = ((part + 1) * M) / iparts;

@@ -234,6 +234,9 @@ struct FieldArgs {
     const double *xw;         // [n]
     int nx, n, M;
     double kappa, dx, length, accel, bfield, umax, vmax, du, dv, courant;
+    // 1: each CTA first copies the phase-table entries it reads in its loops into shared memory
+    // (field_prefetch_bytes more dynamic shared memory; the arithmetic is unchanged)
+    int prefetch;
 };
 
 constexpr int FIELD_THREADS = 1024;            // threads of the single-CTA scalar kernel
