@@ -1,6 +1,6 @@
 """CPU oracle for the 1D2V DG Vlasov-Poisson hot path (NumPy, FP64).
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: ``tests/``, ``__graft_entry__.smoke()``
+TEST INFRASTRUCTURE ONLY.  This module is the oracle: ``tests/``, ``__graft_entry__.smoke()``
 and the CPU-baseline / reference arms of ``bench.py`` may import it.  The product package
 (``vlasov1d2v_b200``) never imports it and has no CPU fallback.
 

@@ -1,5 +1,5 @@
 """The closure MLP's CPU oracle: its backward pass against finite differences (FP64, no bf16
-rounding), so that it can serve as the checker of the GPU kernels."""
+rounding), so that it can serve as the oracle of the GPU kernels."""
 import numpy as np
 
 from oracle import mlp_oracle as mo

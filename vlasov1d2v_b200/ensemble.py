@@ -6,7 +6,7 @@ orders 1..9 and physics) and advances all of them with the native ensemble drive
 and one persistent stage kernel for every member together, K steps captured in one CUDA graph.
 Each member keeps its own loop state, so members with different final times share a batch.
 
-``autotune`` picks the driver's schedule -- threads per CTA, resident CTAs per SM and work
+``autotune`` picks the ensemble's schedule -- threads per CTA, resident CTAs per SM and work
 items per CTA -- by timing candidate schedules on the ensemble itself (states restored
 afterwards), and caches the winner per ensemble signature and GPU in a JSON file.  A schedule
 ``(0, native, items_per_cta)`` is the by-order form (``vl_ens_schedule_by_order``): one stage

@@ -7,8 +7,8 @@
 and ``cupy``, ``matplotlib`` and ``pyvista`` (``main/main.py:1-13``).  ``run_driver`` executes the
 file as it is, with those names resolved to this package's modules (the same classes and call
 signatures), ``cupy`` to ``cupy_compat`` and the two plotting packages to inert stand-ins: the
-script's figures and its 3-D render (``main/main.py:96-110``, ``:180-227``) are skipped, since
-this build is headless.  ``RunData`` writes the run files into the working directory (HDF5 when
+script's figures and its 3-D render (``main/main.py:96-110``, ``:180-227``) are skipped: the
+package has no graphics path.  ``RunData`` writes the run files into the working directory (HDF5 when
 ``h5py`` is importable, raw per-dataset files otherwise).  The script ends with ``quit()``; the
 globals it built (``stepper``, ``f0``, ``e``, ``grids`` ...) are returned.
 """
