@@ -37,12 +37,14 @@ constexpr int FS_THREADS = 256;     // threads per CTA
 // dynamic shared memory of one CTA: C_E and C_P, [n][M] complex each
 __host__ __device__ constexpr size_t field_solve_smem(int n, int M) { return sizeof(double2) * (size_t)2 * n * M; }
 
-// the phase-table entries one CTA reads in its loops: the columns of its modes for every element
-// (forward transform) and the rows of the elements that hold its nodes (inverse transform)
+// the table entries one CTA reads: the phase columns of its modes for every element and the ell
+// columns of its modes (forward transform), the phase rows of the elements that hold its nodes
+// (inverse transform) and the node phases qnode (node-transformed coefficients)
 __host__ __device__ constexpr int field_fwd_cols(int M) { return (M + FC - 1) / FC; }
 __host__ __device__ constexpr int field_inv_rows(int nx, int n) { return ((nx * n + FC - 1) / FC + n - 1) / n + 1; }
 __host__ __device__ constexpr size_t field_prefetch_bytes(int nx, int n, int M) {
-    return sizeof(double2) * ((size_t)nx * field_fwd_cols(M) + (size_t)field_inv_rows(nx, n) * M);
+    return sizeof(double2) * ((size_t)nx * field_fwd_cols(M) + (size_t)field_inv_rows(nx, n) * M +
+                              (size_t)n * field_fwd_cols(M) + (size_t)n * M);
 }
 // dynamic shared memory the loop's field solves may take with the prefetch (the kernel's static
 // shared memory is about 20 KB)
@@ -70,10 +72,6 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     extern __shared__ double2 fs_dyn[];
     const int tid = threadIdx.x;
     const int n = a.n, nx = a.nx, nn = nx * n, M = a.M;
-    // every CTA of the cluster takes the same decision (the loop state is read before any write
-    // of this launch: rank 0 writes only active and dt, the others read active_next)
-    const bool go = field_gate(a, rank == 0);
-    if (!go) return;   // the whole cluster returns: no barrier is left waiting
     double2 *sCE = fs_dyn;
     double2 *sCP = fs_dyn + (size_t)n * M;
     const int Mc = field_fwd_cols(M);
@@ -85,14 +83,28 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     const int e_hi = p0 < nn ? (min(p0 + Nc, nn) - 1) / n : -1;
     double2 *sPF = sCP + (size_t)n * M;            // [nx][Mc]: phase[e][m0 + ml]
     double2 *sPI = sPF + (size_t)nx * Mc;          // [e_hi - e_lo + 1][M]: phase rows of e_lo..e_hi
-    if (a.prefetch) {
+    double2 *sEL = sPI + (size_t)field_inv_rows(nx, n) * M;   // [n][Mc]: ell[j][m0 + ml]
+    double2 *sQN = sEL + (size_t)n * Mc;           // [n][M]: qnode
+    if (a.prefetch) {   // (issued before the gate's read of the loop state, to overlap it)
         for (int q = tid; q < nx * Mc; q += blockDim.x) {
             const int e = q / Mc, ml = q - e * Mc;
             if (m0 + ml < M) field_cp16(sPF + q, a.phase + (size_t)e * M + m0 + ml);
         }
         const int rows = e_hi - e_lo + 1;
         for (int q = tid; q < rows * M; q += blockDim.x) field_cp16(sPI + q, a.phase + (size_t)e_lo * M + q);
+        for (int q = tid; q < n * Mc; q += blockDim.x) {
+            const int j = q / Mc, ml = q - j * Mc;
+            if (m0 + ml < M) field_cp16(sEL + q, a.ell + (size_t)j * M + m0 + ml);
+        }
+        for (int q = tid; q < n * M; q += blockDim.x) field_cp16(sQN + q, a.qnode + q);
         asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+    // every CTA of the cluster takes the same decision (the loop state is read before any write
+    // of this launch: rank 0 writes only active and dt, the others read active_next)
+    const bool go = field_gate(a, rank == 0);
+    if (!go) {   // the whole cluster returns: no barrier is left waiting, no copy in flight
+        if (a.prefetch) asm volatile("cp.async.wait_all;" ::: "memory");
+        return;
     }
 
     // 1. charge (every CTA, identical)
@@ -131,7 +143,8 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
         if (part < parts && m < M) {
             double2 ell[NMAX];
 #pragma unroll
-            for (int j = 0; j < NMAX; ++j) ell[j] = (j < n) ? a.ell[(size_t)j * M + m] : make_double2(0.0, 0.0);
+            for (int j = 0; j < NMAX; ++j)
+                ell[j] = (j < n) ? (a.prefetch ? sEL[j * Mc + ml] : a.ell[(size_t)j * M + m]) : make_double2(0.0, 0.0);
             const int e0 = (part * nx) / parts, e1 = ((part + 1) * nx) / parts;
             for (int e = e0; e < e1; ++e) {
                 double sr = 0.0, si = 0.0;
@@ -182,7 +195,7 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     // 3. node-transformed coefficients of every mode
     for (int q = tid; q < n * M; q += blockDim.x) {
         const int j = q / M, m = q - j * M;
-        const double2 qq = a.qnode[q];
+        const double2 qq = a.prefetch ? sQN[q] : a.qnode[q];
         const double2 Eh = s_E[m], Ph = s_P[m];
         sCE[q] = make_double2(Eh.x * qq.x - Eh.y * qq.y, Eh.x * qq.y + Eh.y * qq.x);
         sCP[q] = make_double2(Ph.x * qq.x - Ph.y * qq.y, Ph.x * qq.y + Ph.y * qq.x);
