@@ -780,18 +780,21 @@ vl::FieldArgs field_args(const vl_ctx *c) {
     a.du = c->cfg.du;
     a.dv = c->cfg.dv;
     a.courant = c->cfg.courant;
-    a.prefetch = vl::field_solve_smem(a.n, a.M) + vl::field_prefetch_bytes(a.nx, a.n, a.M) <= vl::FIELD_DYN_SMEM_MAX;
     return a;
 }
 
 // the whole spectral solve in one thread-block cluster of vl::FC CTAs (vlasov_field.cuh)
-int field(const vl_ctx *c, const vl::FieldArgs &a, cudaStream_t s) {
+int field(const vl_ctx *c, const vl::FieldArgs &a0, cudaStream_t s) {
+    // the table prefetch where it fits the dynamic shared memory budget
+    vl::FieldArgs a = a0;
+    const size_t base = vl::field_solve_smem_for(a.n, a.M, a.phi != nullptr);
+    const size_t pre = vl::field_prefetch_bytes(a.nx, a.n, a.M);
+    a.prefetch = base + pre <= vl::FIELD_DYN_SMEM_MAX ? 1 : 0;
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
     cfg.gridDim = dim3(vl::FC);
     cfg.blockDim = dim3(vl::FS_THREADS);
-    cfg.dynamicSmemBytes = vl::field_solve_smem(c->cfg.n, c->cfg.n_modes) +
-                           (a.prefetch ? vl::field_prefetch_bytes(c->cfg.nx, c->cfg.n, c->cfg.n_modes) : 0);
+    cfg.dynamicSmemBytes = base + (a.prefetch ? pre : 0);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;

@@ -34,8 +34,12 @@ namespace vl {
 constexpr int FC = 8;               // CTAs per cluster (portable cluster size)
 constexpr int FS_THREADS = 256;     // threads per CTA
 
-// dynamic shared memory of one CTA: C_E and C_P, [n][M] complex each
+// dynamic shared memory of one CTA: C_E and C_P, [n][M] complex each (C_P only when phi is asked
+// for: field_solve_smem_for)
 __host__ __device__ constexpr size_t field_solve_smem(int n, int M) { return sizeof(double2) * (size_t)2 * n * M; }
+__host__ __device__ constexpr size_t field_solve_smem_for(int n, int M, bool phi) {
+    return sizeof(double2) * (size_t)(phi ? 2 : 1) * n * M;
+}
 
 // the table entries one CTA reads: the phase columns of its modes for every element and the ell
 // columns of its modes (forward transform), the phase rows of the elements that hold its nodes
@@ -72,6 +76,9 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     extern __shared__ double2 fs_dyn[];
     const int tid = threadIdx.x;
     const int n = a.n, nx = a.nx, nn = nx * n, M = a.M;
+    // phi's node-transformed coefficients only when phi is asked for (the loop's last solve of a
+    // step); the prefetched tables follow
+    const bool want_phi = a.phi != nullptr;
     double2 *sCE = fs_dyn;
     double2 *sCP = fs_dyn + (size_t)n * M;
     const int Mc = field_fwd_cols(M);
@@ -81,7 +88,7 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
     // elements holding this rank's nodes [p0, min(p0 + Nc, nn))
     const int e_lo = p0 < nn ? p0 / n : 0;
     const int e_hi = p0 < nn ? (min(p0 + Nc, nn) - 1) / n : -1;
-    double2 *sPF = sCP + (size_t)n * M;            // [nx][Mc]: phase[e][m0 + ml]
+    double2 *sPF = fs_dyn + (size_t)(want_phi ? 2 : 1) * n * M;   // [nx][Mc]: phase[e][m0 + ml]
     double2 *sPI = sPF + (size_t)nx * Mc;          // [e_hi - e_lo + 1][M]: phase rows of e_lo..e_hi
     double2 *sEL = sPI + (size_t)field_inv_rows(nx, n) * M;   // [n][Mc]: ell[j][m0 + ml]
     double2 *sQN = sEL + (size_t)n * Mc;           // [n][M]: qnode
@@ -198,7 +205,7 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
         const double2 qq = a.prefetch ? sQN[q] : a.qnode[q];
         const double2 Eh = s_E[m], Ph = s_P[m];
         sCE[q] = make_double2(Eh.x * qq.x - Eh.y * qq.y, Eh.x * qq.y + Eh.y * qq.x);
-        sCP[q] = make_double2(Ph.x * qq.x - Ph.y * qq.y, Ph.x * qq.y + Ph.y * qq.x);
+        if (want_phi) sCP[q] = make_double2(Ph.x * qq.x - Ph.y * qq.y, Ph.x * qq.y + Ph.y * qq.x);
     }
     __syncthreads();
 
@@ -215,13 +222,21 @@ __device__ __forceinline__ void field_cluster_body(const FieldArgs &a) {
             const int e = p / n, j = p - e * n;
             const double2 *ph = a.prefetch ? sPI + (size_t)(e - e_lo) * M : a.phase + (size_t)e * M;
             const double2 *ce = sCE + (size_t)j * M;
-            const double2 *cp = sCP + (size_t)j * M;
             const int mb = (part * M) / iparts, me = ((part + 1) * M) / iparts;
+            if (want_phi) {
+                const double2 *cp = sCP + (size_t)j * M;
 #pragma unroll 4
-            for (int m = mb; m < me; ++m) {
-                const double2 h = ph[m];   // Re(conj(h) c) = h.x c.x + h.y c.y
-                er = fma(h.x, ce[m].x, fma(h.y, ce[m].y, er));
-                pr = fma(h.x, cp[m].x, fma(h.y, cp[m].y, pr));
+                for (int m = mb; m < me; ++m) {
+                    const double2 h = ph[m];   // Re(conj(h) c) = h.x c.x + h.y c.y
+                    er = fma(h.x, ce[m].x, fma(h.y, ce[m].y, er));
+                    pr = fma(h.x, cp[m].x, fma(h.y, cp[m].y, pr));
+                }
+            } else {
+#pragma unroll 4
+                for (int m = mb; m < me; ++m) {
+                    const double2 h = ph[m];
+                    er = fma(h.x, ce[m].x, fma(h.y, ce[m].y, er));
+                }
             }
         }
         __syncthreads();
